@@ -1,0 +1,364 @@
+// aux_kernels.cu -- plane-sized work around the stencil: mode sources, mode
+// overlap monitors, running DFTs, probes and the taper edge store/gradient.
+//
+// All of it touches one z-plane (or a list of edge cells) per step, so it is
+// a small fraction of a step's HBM traffic; what matters is that it stays on
+// the device (no per-step host round trip) and that the reductions are FP64.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace fdtd {
+
+// ---------------------------------------------------------------------------
+// Mode plane source, timefield3d_mode_source (timefield3d.c:2977-3026):
+//   src[m<3]  = A ep_m (Re cos(phase) + Im sin(phase))
+//   src[m>=3] = -M_sign A mu_m (Re cos(phase) + Im sin(phase)),  M_sign = 2 reverse - 1
+// from the mode sample at ((int)((i-cx) r) + mi/2, (int)((j-cy) r) + mj/2),
+// r = disc / mode.disc; cells whose sample falls outside the mode keep their
+// value.  Adjoint variant, timefield3d_mode_source_adjoint
+// (timefield3d.c:3028-3068): J = (Hy_m, -Hx_m, 0), M = (-M_sign Ey_m, M_sign Ex_m, 0).
+// cos/sin of the phase are computed on the host with the C library, like the
+// reference, and passed in; sched != null selects per-step values indexed by
+// the device step counter.
+// ---------------------------------------------------------------------------
+__global__ void k_mode_source(float *plane, const float *ep_plane0, const float *ep_plane1, const float *ep_plane2,
+                              const float *mu_plane0, const float *mu_plane1, const float *mu_plane2, int nx,
+                              int ny, int cx, int cy, const double2 *mode, int mi, int mj, double ratio,
+                              double amplitude, double cph, double sph, const double *sched,
+                              const long long *step, int nsched, int reverse, int adjoint)
+{
+    const long long nxy = (long long)nx * ny;
+    double A = amplitude, c = cph, s = sph;
+    if (sched) {
+        long long n = *step;
+        if (n < 0 || n >= nsched) {
+            A = 0.0; c = 0.0; s = 0.0;   // outside the schedule: zero source
+        } else {
+            A = sched[3 * n]; c = sched[3 * n + 1]; s = sched[3 * n + 2];
+        }
+    }
+    const int M_sign = -1 + 2 * reverse;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nxy; t += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(t % nx), j = (int)(t / nx);
+        double xd = dmul((double)(i - cx), ratio);
+        double yd = dmul((double)(j - cy), ratio);
+        int mx = (int)xd + mi / 2, my = (int)yd + mj / 2;
+        if (mx < 0 || mx >= mi || my < 0 || my >= mj) continue;
+        const double2 *e = mode + 6LL * (mx + (long long)mi * my);
+        if (!adjoint) {
+            const float *epp[3] = {ep_plane0, ep_plane1, ep_plane2};
+            const float *mup[3] = {mu_plane0, mu_plane1, mu_plane2};
+#pragma unroll
+            for (int m = 0; m < 6; m++) {
+                double proj = dadd(dmul(e[m].x, c), dmul(e[m].y, s));
+                double v;
+                if (m < 3) v = dmul(dmul(A, (double)epp[m][t]), proj);
+                else v = dmul(dmul(dmul((double)(-M_sign), A), (double)mup[m - 3][t]), proj);
+                plane[m * nxy + t] = __double2float_rn(v);
+            }
+        } else {
+            plane[0 * nxy + t] = __double2float_rn(dmul(1.0, dadd(dmul(e[4].x, c), dmul(e[4].y, s))));
+            plane[1 * nxy + t] = __double2float_rn(dmul(-1.0, dadd(dmul(e[3].x, c), dmul(e[3].y, s))));
+            plane[2 * nxy + t] = 0.0f;
+            plane[3 * nxy + t] = __double2float_rn(dmul((double)(-1 * M_sign), dadd(dmul(e[1].x, c), dmul(e[1].y, s))));
+            plane[4 * nxy + t] = __double2float_rn(dmul((double)(1 * M_sign), dadd(dmul(e[0].x, c), dmul(e[0].y, s))));
+            plane[5 * nxy + t] = 0.0f;
+        }
+    }
+}
+
+__global__ void k_set_value(float *p, long long idx, float v) { p[idx] = v; }
+
+// ---------------------------------------------------------------------------
+// Mode overlap (timefield3d.c:3176-3233): per cell with a mode sample,
+//   Hx mEy - Hy mEx + Ey mHx - Ex mHy   (mode H -> -conj(H) when reverse)
+// summed over the plane in FP64.  One grid covers several monitors
+// (blockIdx.y); each block writes one partial; the finalize kernel adds the
+// partials in a fixed order (deterministic), scales by -dx^2/2 and, for
+// monitors, accumulates e^{i omega n dt} o(n) per frequency with Kahan
+// compensation.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_overlap_partial(const T *const *Ex_, int nx, int ny, const OverlapJob *jobs, double2 *partials,
+                                  int nparts)
+{
+    const OverlapJob jb = jobs[blockIdx.y];
+    const long long nxy = (long long)nx * ny;
+    const T *Ex = Ex_[0], *Ey = Ex_[1], *Hx = Ex_[3], *Hy = Ex_[4];
+    const long long base = nxy * jb.cz;
+    double sre = 0.0, sim = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nxy; t += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(t % nx), j = (int)(t / nx);
+        double xd = dmul((double)(i - jb.cx), jb.ratio);
+        double yd = dmul((double)(j - jb.cy), jb.ratio);
+        int mx = (int)xd + jb.mi / 2, my = (int)yd + jb.mj / 2;
+        if (mx < 0 || mx >= jb.mi || my < 0 || my >= jb.mj) continue;
+        const double2 *e = jb.mode + 6LL * (mx + (long long)jb.mi * my);
+        double2 mEx = e[0], mEy = e[1], mHx = e[3], mHy = e[4];
+        if (jb.reverse) {
+            mHx.x = -mHx.x;
+            mHy.x = -mHy.x;
+        }
+        double ex = (double)Ex[base + t], ey = (double)Ey[base + t];
+        double hx = (double)Hx[base + t], hy = (double)Hy[base + t];
+        double re = dadd(dsub(dmul(hx, mEy.x), dmul(hy, mEx.x)), dsub(dmul(ey, mHx.x), dmul(ex, mHy.x)));
+        double im = dadd(dsub(dmul(hx, mEy.y), dmul(hy, mEx.y)), dsub(dmul(ey, mHx.y), dmul(ex, mHy.y)));
+        sre = dadd(sre, re);
+        sim = dadd(sim, im);
+    }
+    // warp then block reduction, fixed shape
+    for (int o = 16; o > 0; o >>= 1) {
+        sre = dadd(sre, __shfl_down_sync(0xffffffffu, sre, o));
+        sim = dadd(sim, __shfl_down_sync(0xffffffffu, sim, o));
+    }
+    __shared__ double2 ws[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) ws[warp] = make_double2(sre, sim);
+    __syncthreads();
+    if (warp == 0) {
+        int nw = blockDim.x >> 5;
+        double2 v = lane < nw ? ws[lane] : make_double2(0.0, 0.0);
+        for (int o = 16; o > 0; o >>= 1) {
+            v.x = dadd(v.x, __shfl_down_sync(0xffffffffu, v.x, o));
+            v.y = dadd(v.y, __shfl_down_sync(0xffffffffu, v.y, o));
+        }
+        if (lane == 0) partials[(long long)blockIdx.y * nparts + blockIdx.x] = v;
+    }
+}
+
+// reduce_phase: phase - (int)(phase/(2 pi)) 2 pi with the reference's 9-digit pi
+// (timefield3d.c:3,3235)
+__device__ __forceinline__ double reduce_phase(double ph)
+{
+    const double two_pi = dmul(2.0, 3.141592652);
+    double q = (double)(int)__ddiv_rn(ph, two_pi);
+    return dsub(ph, dmul(q, two_pi));
+}
+
+__global__ void k_overlap_finalize(const OverlapJob *jobs, int njobs, const double2 *partials, int nparts,
+                                   double scale, double dt, const long long *step, int step_offset)
+{
+    const int jid = blockIdx.x;
+    if (jid >= njobs) return;
+    const OverlapJob jb = jobs[jid];
+    __shared__ double2 tot;
+    if (threadIdx.x == 0) {
+        double sre = 0.0, sim = 0.0;
+        for (int p = 0; p < nparts; p++) {
+            double2 v = partials[(long long)jid * nparts + p];
+            sre = dadd(sre, v.x);
+            sim = dadd(sim, v.y);
+        }
+        tot = make_double2(dmul(scale, sre), dmul(scale, sim));
+        if (jb.inst) *jb.inst = tot;
+    }
+    __syncthreads();
+    if (!jb.acc) return;
+    const long long n = *step + step_offset;
+    const double2 o = tot;
+    // one thread per frequency: acc[2f] = sum, acc[2f+1] = Kahan compensation
+    for (int f = threadIdx.x; f < jb.nfreq; f += blockDim.x) {
+        double ph = reduce_phase(dmul(dmul((double)n, dt), jb.omega[f]));
+        double s, c;
+        sincos(ph, &s, &c);
+        double add_re = dsub(dmul(c, o.x), dmul(s, o.y));
+        double add_im = dadd(dmul(c, o.y), dmul(s, o.x));
+        double2 sum = jb.acc[2 * f], comp = jb.acc[2 * f + 1];
+        double yr = dsub(add_re, comp.x), yi = dsub(add_im, comp.y);
+        double tr = dadd(sum.x, yr), ti = dadd(sum.y, yi);
+        comp.x = dsub(dsub(tr, sum.x), yr);
+        comp.y = dsub(dsub(ti, sum.y), yi);
+        jb.acc[2 * f] = make_double2(tr, ti);
+        jb.acc[2 * f + 1] = comp;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Running single-frequency DFT (timefield3d.c:2851-2975): acc += f * twiddle,
+// complex double per component; the twiddle is the host-computed
+// e^{i reduced phase} of the reference's power series.  Either the y-slice
+// j = slice (acc indexed [m][k][i]) or the whole grid (acc indexed [m][q]).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_dft(const T *const *f, int nx, int ny, int nz, int slice, int k_lo, int k_hi, double tr,
+                      double ti, double2 *acc)
+{
+    const long long nxy = (long long)nx * ny;
+    long long cnt = slice >= 0 ? (long long)nx * (k_hi - k_lo) : nxy * (k_hi - k_lo);
+    const long long accn = slice >= 0 ? (long long)nx * nz : nxy * nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cnt; t += (long long)gridDim.x * blockDim.x) {
+        long long q, a;
+        if (slice >= 0) {
+            int i = (int)(t % nx);
+            int k = k_lo + (int)(t / nx);
+            q = i + (long long)nx * slice + nxy * k;
+            a = i + (long long)nx * k;
+        } else {
+            q = nxy * k_lo + t;
+            a = q;
+        }
+#pragma unroll
+        for (int m = 0; m < 6; m++) {
+            double v = (double)f[m][q];
+            double2 s = acc[m * accn + a];
+            s.x = dadd(s.x, dmul(v, tr));
+            s.y = dadd(s.y, dmul(v, ti));
+            acc[m * accn + a] = s;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Probes: buf[p*cap + count[p]] = f[m_p][q_p] after each step.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_probes(const T *const *f, const ProbeJob *probes, int np, double *buf, int cap, int *count)
+{
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    int c = count[p];
+    if (c < cap) buf[(long long)p * cap + c] = (double)f[probes[p].m][probes[p].q];
+    count[p] = c + 1;
+}
+
+__global__ void k_step_advance(long long *step) { *step += 1; }
+
+// ---------------------------------------------------------------------------
+// Taper edge store (adjoint3d.c:259-337): gather E (3 components) at the
+// rasterised edge pixels of every (edge, j, k); store[t][cell][3].
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_taper_store(const T *const *f, const long long *cells, int ncell, T *store, int t_index,
+                              const long long *step, int t0, int dir, int duration)
+{
+    int t = t_index;
+    if (step) t = t0 + dir * (int)(*step);
+    if (t < 0 || t >= duration) return;
+    T *dst = store + (long long)t * ncell * 3;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+        long long q = cells[c];
+        dst[3 * c + 0] = f[0][q];
+        dst[3 * c + 1] = f[1][q];
+        dst[3 * c + 2] = f[2][q];
+    }
+}
+
+// ep-gradient, adjoint3d_taper_calculate_ep_gradient (adjoint3d.c:339-373):
+// g[cell] = sum_t sum_{m<3} fwd * adj, FP64, time-ordered like the reference.
+template <typename T>
+__global__ void k_ep_gradient(const T *fwd, const T *adj, int ncell, int duration, double *grad)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    double sum = 0.0;
+    for (int t = 0; t < duration; t++) {
+        const long long o = ((long long)t * ncell + c) * 3;
+#pragma unroll
+        for (int m = 0; m < 3; m++) sum = dadd(sum, dmul((double)fwd[o + m], (double)adj[o + m]));
+    }
+    grad[c] = sum;
+}
+
+// ---------------------------------------------------------------------------
+// materials: finite check (one flag), and FP32 update coefficients
+// ---------------------------------------------------------------------------
+__global__ void k_check_finite(const float *a, long long n, int *bad)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        if (!isfinite(a[q])) { *bad = 1; return; }
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+void launch_mode_source(float *plane, const float *const ep_plane[3], const float *const mu_plane[3], int nx, int ny,
+                        int cx, int cy, const double2 *mode, int mi, int mj, double ratio, double amplitude,
+                        double cph, double sph, const double *sched, const long long *step, int nsched, int reverse,
+                        int adjoint, cudaStream_t st)
+{
+    long long nxy = (long long)nx * ny;
+    int blocks = (int)((nxy + 255) / 256);
+    if (blocks > 1184) blocks = 1184;
+    k_mode_source<<<blocks, 256, 0, st>>>(plane, ep_plane[0], ep_plane[1], ep_plane[2], mu_plane[0], mu_plane[1],
+                                          mu_plane[2], nx, ny, cx, cy, mode, mi, mj, ratio, amplitude, cph, sph, sched,
+                                          step, nsched, reverse, adjoint);
+}
+
+void launch_set_value(float *p, long long idx, float v, cudaStream_t st) { k_set_value<<<1, 1, 0, st>>>(p, idx, v); }
+
+int overlap_parts(int nx, int ny)
+{
+    long long nxy = (long long)nx * ny;
+    long long b = (nxy + 255) / 256;
+    return (int)(b < 64 ? b : 64);
+}
+
+template <typename T>
+void launch_overlap(const T *const *f_dev, int nx, int ny, const OverlapJob *jobs_dev, int njobs, double2 *partials,
+                    double scale, double dt, const long long *step, int step_offset, cudaStream_t st)
+{
+    if (njobs <= 0) return;
+    int parts = overlap_parts(nx, ny);
+    k_overlap_partial<T><<<dim3(parts, njobs), 256, 0, st>>>(f_dev, nx, ny, jobs_dev, partials, parts);
+    k_overlap_finalize<<<njobs, 32, 0, st>>>(jobs_dev, njobs, partials, parts, scale, dt, step, step_offset);
+}
+
+template <typename T>
+void launch_dft(const T *const *f_dev, int nx, int ny, int nz, int slice, int k_lo, int k_hi, double tr, double ti,
+                double2 *acc, cudaStream_t st)
+{
+    if (k_hi <= k_lo) return;
+    long long cnt = slice >= 0 ? (long long)nx * (k_hi - k_lo) : (long long)nx * ny * (k_hi - k_lo);
+    int blocks = (int)((cnt + 255) / 256);
+    if (blocks > 4736) blocks = 4736;
+    k_dft<T><<<blocks, 256, 0, st>>>(f_dev, nx, ny, nz, slice, k_lo, k_hi, tr, ti, acc);
+}
+
+template <typename T>
+void launch_probes(const T *const *f_dev, const ProbeJob *probes, int np, double *buf, int cap, int *count,
+                   cudaStream_t st)
+{
+    if (np <= 0) return;
+    k_probes<T><<<(np + 127) / 128, 128, 0, st>>>(f_dev, probes, np, buf, cap, count);
+}
+
+void launch_step_advance(long long *step, cudaStream_t st) { k_step_advance<<<1, 1, 0, st>>>(step); }
+
+template <typename T>
+void launch_taper_store(const T *const *f_dev, const long long *cells, int ncell, T *store, int t_index,
+                        const long long *step, int t0, int dir, int duration, cudaStream_t st)
+{
+    if (ncell <= 0) return;
+    int blocks = (ncell + 255) / 256;
+    if (blocks > 592) blocks = 592;
+    k_taper_store<T><<<blocks, 256, 0, st>>>(f_dev, cells, ncell, store, t_index, step, t0, dir, duration);
+}
+
+template <typename T>
+void launch_ep_gradient(const T *fwd, const T *adj, int ncell, int duration, double *grad, cudaStream_t st)
+{
+    if (ncell <= 0) return;
+    k_ep_gradient<T><<<(ncell + 127) / 128, 128, 0, st>>>(fwd, adj, ncell, duration, grad);
+}
+
+void launch_check_finite(const float *a, long long n, int *bad, cudaStream_t st)
+{
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 2368) blocks = 2368;
+    if (blocks > 0) k_check_finite<<<blocks, 256, 0, st>>>(a, n, bad);
+}
+
+#define FDTD_INST(T)                                                                                               \
+    template void launch_overlap<T>(const T *const *, int, int, const OverlapJob *, int, double2 *, double, double, \
+                                    const long long *, int, cudaStream_t);                                         \
+    template void launch_dft<T>(const T *const *, int, int, int, int, int, int, double, double, double2 *,         \
+                                cudaStream_t);                                                                     \
+    template void launch_probes<T>(const T *const *, const ProbeJob *, int, double *, int, int *, cudaStream_t);   \
+    template void launch_taper_store<T>(const T *const *, const long long *, int, T *, int, const long long *, int, \
+                                        int, int, cudaStream_t);                                                   \
+    template void launch_ep_gradient<T>(const T *, const T *, int, int, double *, cudaStream_t);
+FDTD_INST(float)
+FDTD_INST(double)
+#undef FDTD_INST
+
+}  // namespace fdtd

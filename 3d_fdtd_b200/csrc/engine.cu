@@ -1,0 +1,1014 @@
+// engine.cu -- device state of grids, modes and tapers; the step sequence;
+// CUDA-graph capture of multi-step runs.
+#include "engine.h"
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <unordered_map>
+
+namespace fdtd {
+
+// ============================================================================
+// status
+// ============================================================================
+static thread_local int t_err = FDTD_OK;
+static thread_local char t_msg[512] = "";
+
+void set_error(int code, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(t_msg, sizeof t_msg, fmt, ap);
+    va_end(ap);
+    t_err = code;
+    fprintf(stderr, "libfdtd_b200: error %d: %s\n", code, t_msg);
+}
+}  // namespace fdtd
+
+extern "C" int fdtd_last_error(void) { return fdtd::t_err; }
+extern "C" const char *fdtd_last_error_message(void) { return fdtd::t_msg; }
+extern "C" void fdtd_clear_error(void)
+{
+    fdtd::t_err = FDTD_OK;
+    fdtd::t_msg[0] = 0;
+}
+
+namespace fdtd {
+
+bool cuda_ok(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return true;
+    set_error(e == cudaErrorMemoryAllocation ? FDTD_ERR_ALLOC : FDTD_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return false;
+}
+
+#define CK(call)                                   \
+    do {                                           \
+        if (!cuda_ok((call), #call)) return false; \
+    } while (0)
+#define CKL(what)                                        \
+    do {                                                 \
+        if (!cuda_ok(cudaGetLastError(), what)) return false; \
+    } while (0)
+
+bool device_available()
+{
+    static int state = -1;   // -1 unknown, 0 none, 1 ok
+    static std::string why;
+    if (state < 0) {
+        int n = 0;
+        cudaError_t e = cudaGetDeviceCount(&n);
+        if (e != cudaSuccess || n == 0) {
+            state = 0;
+            why = e != cudaSuccess ? cudaGetErrorString(e) : "no CUDA device";
+        } else {
+            state = 1;
+        }
+    }
+    if (state == 0) {
+        set_error(FDTD_ERR_NO_DEVICE, "no usable CUDA device (%s); this library has no CPU fallback", why.c_str());
+        return false;
+    }
+    return true;
+}
+
+std::mutex &api_mutex()
+{
+    static std::mutex m;
+    return m;
+}
+
+template <typename P> static bool dalloc(P **p, size_t bytes, cudaStream_t st, bool zero = true)
+{
+    if (*p) return true;
+    void *v = nullptr;
+    if (!cuda_ok(cudaMalloc(&v, bytes ? bytes : 16), "cudaMalloc")) return false;
+    *p = (P *)v;
+    if (zero) return cuda_ok(cudaMemsetAsync(v, 0, bytes ? bytes : 16, st), "cudaMemsetAsync");
+    return true;
+}
+
+template <typename P> static void dfree(P *&p)
+{
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+
+// ============================================================================
+// modes
+// ============================================================================
+static std::unordered_map<const void *, DevMode *> &mode_table()
+{
+    static std::unordered_map<const void *, DevMode *> t;
+    return t;
+}
+
+static uint64_t mode_fingerprint(const mode &m)
+{
+    // FNV-1a over the dimensions and up to 257 evenly spaced complex entries:
+    // catches a mode rescaled in place (mode_smul) or replaced at the same
+    // address, at O(1) cost per call.
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](const void *p, size_t n) {
+        const unsigned char *c = (const unsigned char *)p;
+        for (size_t i = 0; i < n; i++) { h ^= c[i]; h *= 1099511628211ull; }
+    };
+    mix(&m.i, sizeof m.i);
+    mix(&m.j, sizeof m.j);
+    mix(&m.disc, sizeof m.disc);
+    long long n = 6LL * m.i * m.j;
+    if (n <= 0 || !m.fields.m) return h;
+    const int samples = 257;
+    for (int s = 0; s < samples; s++) {
+        long long q = (n - 1) * s / (samples - 1);
+        mix(&m.fields.m[q], sizeof(complex));
+    }
+    return h;
+}
+
+double mode_power_norm_host(const mode &m)
+{
+    // mode_power_inner_product(psi, psi) (mode.c:1267-1310) and mode_power_norm (1330-1337)
+    double sre = 0, sim = 0;
+    for (int i = 0; i < m.i; i++)
+        for (int j = 0; j < m.j; j++) {
+            const complex *e = m.fields.m + 6 * (size_t)(i + j * m.i);
+            double Exr = e[0].re, Exi = e[0].im, Eyr = e[1].re, Eyi = e[1].im;
+            double Hxr = e[3].re, Hxi = e[3].im, Hyr = e[4].re, Hyi = e[4].im;
+            double p1r = Hxr * Eyr - (-Hxi) * Eyi, p1i = Hxr * Eyi + (-Hxi) * Eyr;
+            double q2r = Hyr * Exr - (-Hyi) * Exi, q2i = Hyr * Exi + (-Hyi) * Exr;
+            double p3r = Hxr * Eyr - Hxi * (-Eyi), p3i = Hxr * (-Eyi) + Hxi * Eyr;
+            double q4r = Hyr * Exr - Hyi * (-Exi), q4i = Hyr * (-Exi) + Hyi * Exr;
+            sre = sre + ((p1r + (0 - q2r)) + (p3r + (0 - q4r)));
+            sim = sim + ((p1i + (0 - q2i)) + (p3i + (0 - q4i)));
+        }
+    double s = (-0.5 * m.disc * m.disc);
+    sre = s * sre;
+    sim = s * sim;
+    return std::sqrt(std::sqrt(sre * sre + sim * sim));
+}
+
+void mode_power_normalize_host(const mode &m)
+{
+    // mode_power_normalize (mode.c:1367-1379): fields *= 1/norm, in place
+    double divisor = 1.0 / mode_power_norm_host(m);
+    size_t n = 6 * (size_t)m.i * m.j;
+    for (size_t q = 0; q < n; q++) {
+        m.fields.m[q].re = divisor * m.fields.m[q].re;
+        m.fields.m[q].im = divisor * m.fields.m[q].im;
+    }
+}
+
+static uint64_t g_mode_version = 1;
+
+DevMode *mode_device(const mode &m)
+{
+    if (m.i <= 0 || m.j <= 0 || !m.fields.m || !(m.disc > 0)) {
+        set_error(FDTD_ERR_ARG, "invalid mode (i=%d j=%d disc=%g)", m.i, m.j, m.disc);
+        return nullptr;
+    }
+    auto &tab = mode_table();
+    const void *key = m.fields.m;
+    uint64_t fp = mode_fingerprint(m);
+    auto it = tab.find(key);
+    if (it != tab.end() && it->second->fingerprint == fp && it->second->mi == m.i && it->second->mj == m.j &&
+        it->second->disc == m.disc)
+        return it->second;
+    // first sight (or changed): power-normalise the caller's mode in place,
+    // as the reference's source/overlap calls do, and upload it
+    mode_power_normalize_host(m);
+    DevMode *dm;
+    if (it == tab.end()) {
+        dm = new DevMode();
+        dm->key = key;
+        tab[key] = dm;
+    } else {
+        dm = it->second;
+        // queued kernels may still read the old copy
+        if (!cuda_ok(cudaDeviceSynchronize(), "cudaDeviceSynchronize")) return nullptr;
+        if (dm->mi != m.i || dm->mj != m.j) dfree(dm->d);
+    }
+    dm->mi = m.i;
+    dm->mj = m.j;
+    dm->disc = m.disc;
+    dm->fingerprint = mode_fingerprint(m);
+    size_t bytes = 6 * (size_t)m.i * m.j * sizeof(double2);
+    if (!dm->d && !cuda_ok(cudaMalloc(&dm->d, bytes), "cudaMalloc(mode)")) return nullptr;
+    if (!cuda_ok(cudaMemcpy(dm->d, m.fields.m, bytes, cudaMemcpyHostToDevice), "cudaMemcpy(mode)")) return nullptr;
+    g_mode_version++;
+    return dm;
+}
+
+void mode_release(const void *key)
+{
+    auto &tab = mode_table();
+    auto it = tab.find(key);
+    if (it == tab.end()) return;
+    cudaDeviceSynchronize();
+    dfree(it->second->d);
+    delete it->second;
+    tab.erase(it);
+    g_mode_version++;
+}
+
+// private normalised device copy of a mode (monitors, schedules)
+static double2 *mode_private_copy(const mode &m)
+{
+    if (m.i <= 0 || m.j <= 0 || !m.fields.m || !(m.disc > 0)) {
+        set_error(FDTD_ERR_ARG, "invalid mode (i=%d j=%d disc=%g)", m.i, m.j, m.disc);
+        return nullptr;
+    }
+    mode_power_normalize_host(m);
+    size_t bytes = 6 * (size_t)m.i * m.j * sizeof(double2);
+    double2 *d = nullptr;
+    if (!cuda_ok(cudaMalloc(&d, bytes), "cudaMalloc(mode)")) return nullptr;
+    if (!cuda_ok(cudaMemcpy(d, m.fields.m, bytes, cudaMemcpyHostToDevice), "cudaMemcpy(mode)")) {
+        cudaFree(d);
+        return nullptr;
+    }
+    return d;
+}
+
+// monitors and schedules keep their own mode copies: key -> (device ptr, dims)
+struct PrivMode {
+    double2 *d;
+    int mi, mj;
+    double disc;
+};
+static std::unordered_map<const void *, PrivMode> &priv_modes()
+{
+    static std::unordered_map<const void *, PrivMode> t;
+    return t;
+}
+static uint64_t g_priv_id = 1;
+
+const void *priv_mode_new(const mode &m)
+{
+    double2 *d = mode_private_copy(m);
+    if (!d) return nullptr;
+    const void *key = (const void *)(uintptr_t)(g_priv_id++);
+    priv_modes()[key] = PrivMode{d, m.i, m.j, m.disc};
+    return key;
+}
+
+void priv_mode_free(const void *key)
+{
+    auto &t = priv_modes();
+    auto it = t.find(key);
+    if (it == t.end()) return;
+    cudaFree(it->second.d);
+    t.erase(it);
+}
+
+// ============================================================================
+// grids
+// ============================================================================
+static std::unordered_map<const void *, Grid *> &grid_table()
+{
+    static std::unordered_map<const void *, Grid *> t;
+    return t;
+}
+
+Grid *grid_lookup(const timefield3d &psi, bool quiet)
+{
+    auto &t = grid_table();
+    auto it = t.find(psi.fields);
+    if (it == t.end()) {
+        if (!quiet) set_error(FDTD_ERR_ARG, "unknown grid (not created by timefield3d_new of this library)");
+        return nullptr;
+    }
+    return it->second;
+}
+
+Grid *grid_register(const timefield3d &psi)
+{
+    Grid *g = new Grid();
+    g->h = psi;
+    g->nx = psi.i;
+    g->ny = psi.j;
+    g->nz = psi.k;
+    g->n = (long long)psi.i * psi.j * psi.k;
+    g->dx = psi.disc;
+    grid_table()[psi.fields] = g;
+    return g;
+}
+
+void grid_unregister(const timefield3d &psi)
+{
+    auto &t = grid_table();
+    auto it = t.find(psi.fields);
+    if (it == t.end()) return;
+    delete it->second;
+    t.erase(it);
+}
+
+static size_t esize(const Grid *g) { return g->prec == FDTD_F64 ? sizeof(double) : sizeof(float); }
+
+static void free_fields(Grid *g)
+{
+    for (int s = 0; s < 2; s++) {
+        for (int m = 0; m < 6; m++) dfree(g->f[s][m]);
+        dfree(g->d_fptr[s]);
+    }
+    for (int m = 0; m < 6; m++) dfree(g->old[m]);
+    for (int s = 0; s < 2; s++)
+        for (int a = 0; a < 3; a++)
+            for (int w = 0; w < 4; w++) dfree(g->psi[s][a][w]);
+    for (int w = 0; w < 6; w++)
+        for (int a = 0; a < 3; a++) dfree(g->prof[w][a]);
+    g->prof_dt = 0;
+    g->cur = 0;
+}
+
+Grid::~Grid()
+{
+    if (dev) {
+        cudaStreamSynchronize(st);
+        if (graph) cudaGraphExecDestroy(graph);
+        free_fields(this);
+        for (int c = 0; c < 3; c++) { dfree(ep[c]); dfree(mu[c]); dfree(cb[c]); dfree(ca[c]); }
+        for (int m = 0; m < 6; m++) dfree(sig[m]);
+        for (auto &p : planes) dfree(p.p);
+        for (auto p : plane_pool) dfree(p);
+        dfree(d_step); dfree(d_jobs); dfree(d_job1); dfree(d_partials); dfree(d_inst);
+        if (h_inst) cudaFreeHost(h_inst);
+        if (h_flag) cudaFreeHost(h_flag);
+        dfree(d_flag);
+        for (auto &mn : monitors) { dfree(mn.d_omega); dfree(mn.d_acc); priv_mode_free(mn.mode_key); }
+        dfree(d_probes); dfree(d_probe_buf); dfree(d_probe_count);
+        dfree(d_dft_full);
+        for (auto &kv : d_dft_slice) dfree(kv.second);
+        if (sched.active) { dfree(sched.d_sched); priv_mode_free(sched.mode_key); }
+        dfree(d_aos);
+        cudaStreamDestroy(st);
+    }
+}
+
+template <typename T> GridView<T> view(Grid *g, int set)
+{
+    GridView<T> v;
+    v.nx = g->nx; v.ny = g->ny; v.nz = g->nz; v.n = g->n;
+    for (int m = 0; m < 6; m++) { v.f[m] = (T *)g->f[set][m]; v.old[m] = (T *)g->old[m]; v.sig[m] = g->sig[m]; }
+    for (int c = 0; c < 3; c++) { v.ep[c] = g->ep[c]; v.mu[c] = g->mu[c]; }
+    return v;
+}
+template GridView<float> view<float>(Grid *, int);
+template GridView<double> view<double>(Grid *, int);
+
+template <typename T> CpmlView<T> cpml_view(Grid *g, int in_set)
+{
+    CpmlView<T> c{};
+    c.L = g->boundary == FDTD_BOUNDARY_CPML ? g->L : 0;
+    for (int a = 0; a < 3; a++) {
+        for (int w = 0; w < 4; w++) c.psi[a][w] = (T *)g->psi[in_set][a][w];
+        for (int w = 0; w < 6; w++) c.prof[w][a] = (const T *)g->prof[w][a];
+    }
+    return c;
+}
+template CpmlView<float> cpml_view<float>(Grid *, int);
+template CpmlView<double> cpml_view<double>(Grid *, int);
+
+SourcePlanes source_table(Grid *g)
+{
+    SourcePlanes s{};
+    s.n = (int)g->planes.size();
+    for (int i = 0; i < s.n; i++) { s.k[i] = g->planes[i].k; s.p[i] = g->planes[i].p; }
+    return s;
+}
+
+// deinterleave AoS float (stride s) into up to 6 SoA arrays; per component c
+// flag[c] bit 1 = some value differs from `ref`, bit 2 = some value is not finite
+__global__ void k_deinterleave(const float *aos, int stride, float *d0, float *d1, float *d2, float *d3, float *d4,
+                               float *d5, long long n, float ref, int *flag)
+{
+    float *d[6] = {d0, d1, d2, d3, d4, d5};
+    int local[6] = {0, 0, 0, 0, 0, 0};
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            if (c >= stride) break;
+            float v = aos[q * stride + c];
+            d[c][q] = v;
+            if (v != ref) local[c] |= 1;
+            if (!isfinite(v)) local[c] |= 2;
+        }
+    }
+    for (int c = 0; c < stride; c++)
+        if (local[c]) atomicOr(flag + c, local[c]);
+}
+
+static bool upload_deinterleave(Grid *g, const float *host, int stride, float **dst, float ref, int *d_flags)
+{
+    size_t bytes = (size_t)g->n * stride * sizeof(float);
+    if (!dalloc(&g->d_aos, (size_t)g->n * 6 * sizeof(double), g->st, false)) return false;
+    CK(cudaMemcpyAsync(g->d_aos, host, bytes, cudaMemcpyHostToDevice, g->st));
+    float *d[6] = {};
+    for (int c = 0; c < stride; c++) d[c] = dst[c];
+    int blocks = (int)std::min<long long>((g->n + 255) / 256, 4736);
+    k_deinterleave<<<blocks, 256, 0, g->st>>>((const float *)g->d_aos, stride, d[0], d[1], d[2], d[3], d[4], d[5],
+                                                g->n, ref, d_flags);
+    CKL("k_deinterleave");
+    return true;
+}
+
+bool grid_upload_materials(Grid *g)
+{
+    // flags: [0..2] ep != 1, [3..5] mu != 1, [6..11] sig != 0 (bit 2: not finite)
+    CK(cudaMemsetAsync(g->d_flag, 0, 12 * sizeof(int), g->st));
+    if (!upload_deinterleave(g, g->h.ep, 3, g->ep, 1.0f, g->d_flag + 0)) return false;
+    if (!upload_deinterleave(g, g->h.mu, 3, g->mu, 1.0f, g->d_flag + 3)) return false;
+    if (!upload_deinterleave(g, g->h.sig, 6, g->sig, 0.0f, g->d_flag + 6)) return false;
+    CK(cudaMemcpyAsync(g->h_flag, g->d_flag, 12 * sizeof(int), cudaMemcpyDeviceToHost, g->st));
+    CK(cudaStreamSynchronize(g->st));
+    int any = 0;
+    for (int c = 0; c < 12; c++) any |= g->h_flag[c];
+    if (any & 2) {
+        set_error(FDTD_ERR_NONFINITE, "non-finite permittivity, permeability or conductivity");
+        return false;
+    }
+    g->mu_nonunit = ((g->h_flag[3] | g->h_flag[4] | g->h_flag[5]) & 1) != 0;
+    g->sig_e = ((g->h_flag[6] | g->h_flag[7] | g->h_flag[8]) & 1) != 0;
+    g->sig_m = ((g->h_flag[9] | g->h_flag[10] | g->h_flag[11]) & 1) != 0;
+    g->mat_dirty = false;
+    g->coef_valid = false;
+    g->version++;
+    return true;
+}
+
+bool grid_upload_fields(Grid *g)
+{
+    if (!dalloc(&g->d_aos, (size_t)g->n * 6 * sizeof(double), g->st, false)) return false;
+    CK(cudaMemcpyAsync(g->d_aos, g->h.fields, (size_t)g->n * 6 * sizeof(double), cudaMemcpyHostToDevice, g->st));
+    if (g->prec == FDTD_F64) launch_aos_to_soa<double>(g->d_aos, (double *const *)g->f[g->cur], g->n, g->st);
+    else launch_aos_to_soa<float>(g->d_aos, (float *const *)g->f[g->cur], g->n, g->st);
+    CKL("aos_to_soa");
+    g->fields_from_host = false;
+    return true;
+}
+
+bool grid_download_fields(Grid *g)
+{
+    if (!dalloc(&g->d_aos, (size_t)g->n * 6 * sizeof(double), g->st, false)) return false;
+    if (g->prec == FDTD_F64) launch_soa_to_aos<double>(g->d_aos, (double *const *)g->f[g->cur], g->n, g->st);
+    else launch_soa_to_aos<float>(g->d_aos, (float *const *)g->f[g->cur], g->n, g->st);
+    CKL("soa_to_aos");
+    CK(cudaMemcpyAsync(g->h.fields, g->d_aos, (size_t)g->n * 6 * sizeof(double), cudaMemcpyDeviceToHost, g->st));
+    CK(cudaStreamSynchronize(g->st));
+    return true;
+}
+
+static bool alloc_field_set(Grid *g, int s)
+{
+    size_t bytes = (size_t)g->n * esize(g);
+    for (int m = 0; m < 6; m++)
+        if (!dalloc(&g->f[s][m], bytes, g->st)) return false;
+    if (!dalloc(&g->d_fptr[s], 6 * sizeof(void *), g->st, false)) return false;
+    CK(cudaMemcpyAsync(g->d_fptr[s], g->f[s], 6 * sizeof(void *), cudaMemcpyHostToDevice, g->st));
+    CK(cudaStreamSynchronize(g->st));
+    return true;
+}
+
+bool grid_ensure_device(Grid *g)
+{
+    if (!device_available()) return false;
+    if (!g->dev) {
+        if (g->nx < 4 || g->ny < 4 || g->nz < 4) {
+            set_error(FDTD_ERR_ARG, "grid %dx%dx%d: every dimension must be >= 4", g->nx, g->ny, g->nz);
+            return false;
+        }
+        CK(cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking));
+        g->dev = true;
+        size_t fb = (size_t)g->n * sizeof(float);
+        for (int c = 0; c < 3; c++) {
+            if (!dalloc(&g->ep[c], fb, g->st, false) || !dalloc(&g->mu[c], fb, g->st, false)) return false;
+        }
+        for (int m = 0; m < 6; m++)
+            if (!dalloc(&g->sig[m], fb, g->st, false)) return false;
+        if (!dalloc(&g->d_step, sizeof(long long), g->st)) return false;
+        if (!dalloc(&g->d_flag, 12 * sizeof(int), g->st)) return false;
+        CK(cudaMallocHost(&g->h_flag, 12 * sizeof(int)));
+        CK(cudaMallocHost(&g->h_inst, sizeof(double2)));
+        if (!dalloc(&g->d_inst, sizeof(double2), g->st)) return false;
+        if (!dalloc(&g->d_job1, sizeof(OverlapJob), g->st)) return false;
+        g->jobs_cap = 8;
+        if (!dalloc(&g->d_jobs, g->jobs_cap * sizeof(OverlapJob), g->st, false)) return false;
+        if (!dalloc(&g->d_partials, (size_t)g->jobs_cap * overlap_parts(g->nx, g->ny) * sizeof(double2), g->st, false))
+            return false;
+        // pin the host mirrors the engine transfers (best effort)
+        cudaHostRegister(g->h.ep, (size_t)g->n * 3 * sizeof(float), cudaHostRegisterDefault);
+        cudaHostRegister(g->h.mu, (size_t)g->n * 3 * sizeof(float), cudaHostRegisterDefault);
+        cudaHostRegister(g->h.sig, (size_t)g->n * 6 * sizeof(float), cudaHostRegisterDefault);
+        cudaGetLastError();
+        g->mat_dirty = true;
+    }
+    if (!g->f[0][0]) {
+        if (!alloc_field_set(g, 0)) return false;
+        g->cur = 0;
+    }
+    if (g->mat_dirty && !grid_upload_materials(g)) return false;
+    if (g->fields_from_host && !grid_upload_fields(g)) return false;
+    return true;
+}
+
+bool grid_set_precision(Grid *g, int prec)
+{
+    if (prec != FDTD_F64 && prec != FDTD_F32) {
+        set_error(FDTD_ERR_ARG, "precision %d", prec);
+        return false;
+    }
+    if (prec == g->prec) return true;
+    if (g->dev && g->f[0][0]) {
+        if (!grid_download_fields(g)) return false;
+        free_fields(g);
+        g->fields_from_host = true;
+    }
+    g->prec = prec;
+    g->coef_valid = false;
+    g->version++;
+    return true;
+}
+
+// CPML profiles along each axis, for step dt.  Depth fraction rho of an E node
+// (p = i) or H node (p = i + 1/2): (L - 1/2 - p)/L on the low side,
+// (p - (N - L - 1/2))/L on the high side; sigma = smax rho^m,
+// kappa = 1 + (kmax - 1) rho^m, alpha = amax (1 - rho),
+// b = exp(-(sigma/kappa + alpha) dt), a = sigma (b - 1)/(sigma kappa + kappa^2 alpha).
+// Computed in double on the host (the CPU restatement uses the same code), so
+// the FP64 path sees identical tables.
+static void cpml_point(double rho, int order, double smax, double kmax, double amax, double dt, double *b, double *a,
+                       double *kinv)
+{
+    if (rho <= 0) { *b = 1.0; *a = 0.0; *kinv = 1.0; return; }
+    double r = std::pow(rho, order);
+    double sigma = smax * r;
+    double kappa = 1.0 + (kmax - 1.0) * r;
+    double alpha = amax * (1.0 - rho);
+    *b = std::exp(-(sigma / kappa + alpha) * dt);
+    *a = sigma > 0 ? sigma * (*b - 1.0) / (sigma * kappa + kappa * kappa * alpha) : 0.0;
+    *kinv = 1.0 / kappa;
+}
+
+static bool build_profiles(Grid *g, double dt)
+{
+    const int L = g->L;
+    double smax = g->smax > 0 ? g->smax : 0.8 * (g->order + 1) / g->dx;
+    int dims[3] = {g->nx, g->ny, g->nz};
+    for (int a = 0; a < 3; a++) {
+        int N = dims[a];
+        std::vector<double> tab[6];
+        for (int w = 0; w < 6; w++) tab[w].resize(N);
+        for (int i = 0; i < N; i++)
+            for (int h = 0; h < 2; h++) {
+                double p = i + 0.5 * h;
+                double rho = 0;
+                if (p < L - 0.5) rho = (L - 0.5 - p) / L;
+                else if (p > N - L - 0.5) rho = (p - (N - L - 0.5)) / L;
+                cpml_point(rho, g->order, smax, g->kmax, g->amax, dt, &tab[3 * h][i], &tab[3 * h + 1][i],
+                           &tab[3 * h + 2][i]);
+            }
+        for (int w = 0; w < 6; w++) {
+            if (!dalloc(&g->prof[w][a], N * sizeof(double), g->st, false)) return false;
+            // ordered on the grid's stream: queued steps still read the old tables
+            // (pageable source: the copy is staged before the call returns)
+            if (g->prec == FDTD_F64) {
+                CK(cudaMemcpyAsync(g->prof[w][a], tab[w].data(), N * sizeof(double), cudaMemcpyHostToDevice, g->st));
+            } else {
+                std::vector<float> f(N);
+                for (int i = 0; i < N; i++) f[i] = (float)tab[w][i];
+                CK(cudaMemcpyAsync(g->prof[w][a], f.data(), N * sizeof(float), cudaMemcpyHostToDevice, g->st));
+            }
+        }
+    }
+    g->prof_dt = dt;
+    return true;
+}
+
+static bool fused_path(const Grid *g)
+{
+    return g->prec == FDTD_F32 && g->boundary != FDTD_BOUNDARY_MUR && !g->sig_m && !g->mu_nonunit &&
+           fused_supported(g->nx, g->ny, g->nz);
+}
+
+// FP32 E-update coefficients of the fused path: cb = main/dx, ca = main*coef,
+// main = 1/(ep/dt + sig/2), coef = ep/dt - sig/2, computed in double.
+__global__ void k_coef(const float *ep, const float *sig, float *cb, float *ca, long long n, double dt, double dx)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        double e = ep[q], s = sig ? sig[q] : 0.0;
+        double main_coeff = 1.0 / (e / dt + 0.5 * s);
+        cb[q] = (float)(main_coeff / dx);
+        if (ca) ca[q] = (float)(main_coeff * (e / dt - 0.5 * s));
+    }
+}
+
+bool grid_prepare_step(Grid *g, double dt)
+{
+    if (!grid_ensure_device(g)) return false;
+    if (!(dt > 0) || !std::isfinite(dt)) {
+        set_error(FDTD_ERR_ARG, "delta_t must be positive and finite (got %g)", dt);
+        return false;
+    }
+    const bool fused = fused_path(g);
+    if (g->boundary == FDTD_BOUNDARY_MUR) {
+        size_t bytes = (size_t)g->n * esize(g);
+        for (int m = 0; m < 6; m++)
+            if (!dalloc(&g->old[m], bytes, g->st)) return false;
+    }
+    if (g->boundary == FDTD_BOUNDARY_CPML) {
+        if (g->L <= 0) {
+            set_error(FDTD_ERR_ARG, "CPML boundary selected without timefield3d_set_cpml");
+            return false;
+        }
+        if (2 * g->L + 2 > g->nx || 2 * g->L + 2 > g->ny || 2 * g->L + 2 > g->nz) {
+            set_error(FDTD_ERR_ARG, "CPML thickness %d too large for grid %dx%dx%d", g->L, g->nx, g->ny, g->nz);
+            return false;
+        }
+        size_t L2 = 2 * (size_t)g->L, es = esize(g);
+        size_t sz[3] = {L2 * g->ny * g->nz * es, (size_t)g->nx * L2 * g->nz * es, (size_t)g->nx * g->ny * L2 * es};
+        for (int s = 0; s < (fused ? 2 : 1); s++)
+            for (int a = 0; a < 3; a++)
+                for (int w = 0; w < 4; w++)
+                    if (!dalloc(&g->psi[s][a][w], sz[a], g->st)) return false;
+        if (g->prof_dt != dt && !build_profiles(g, dt)) return false;
+    }
+    if (fused) {
+        if (!g->f[1][0] && !alloc_field_set(g, 1)) return false;
+        if (!g->coef_valid || g->coef_dt != dt) {
+            size_t fb = (size_t)g->n * sizeof(float);
+            for (int c = 0; c < 3; c++) {
+                if (!dalloc(&g->cb[c], fb, g->st, false)) return false;
+                if (g->sig_e && !dalloc(&g->ca[c], fb, g->st, false)) return false;
+                int blocks = (int)std::min<long long>((g->n + 255) / 256, 4736);
+                k_coef<<<blocks, 256, 0, g->st>>>(g->ep[c], g->sig_e ? g->sig[c] : nullptr, g->cb[c],
+                                                    g->sig_e ? g->ca[c] : nullptr, g->n, dt, g->dx);
+                CKL("k_coef");
+            }
+            g->coef_valid = true;
+            g->coef_dt = dt;
+        }
+    }
+    // overlap scratch for the monitors
+    int parts = overlap_parts(g->nx, g->ny);
+    int need = std::max<int>(1, (int)g->monitors.size());
+    if (g->jobs_cap < need) {
+        dfree(g->d_jobs);
+        dfree(g->d_partials);
+        g->jobs_cap = std::max(need, 8);
+    }
+    if (!dalloc(&g->d_jobs, g->jobs_cap * sizeof(OverlapJob), g->st, false)) return false;
+    if (!dalloc(&g->d_partials, (size_t)g->jobs_cap * parts * sizeof(double2), g->st, false)) return false;
+    return true;
+}
+
+Plane *grid_plane(Grid *g, int k, bool create)
+{
+    for (auto &p : g->planes)
+        if (p.k == k) return &p;
+    if (!create) return nullptr;
+    if ((int)g->planes.size() >= kMaxSourcePlanes) {
+        set_error(FDTD_ERR_UNSUPPORTED, "more than %d z-planes hold sources (zero the grid to reset them)",
+                  kMaxSourcePlanes);
+        return nullptr;
+    }
+    size_t bytes = 6 * (size_t)g->nx * g->ny * sizeof(float);
+    float *p = nullptr;
+    if (!g->plane_pool.empty()) {
+        p = g->plane_pool.back();
+        g->plane_pool.pop_back();
+    } else if (!cuda_ok(cudaMalloc(&p, bytes), "cudaMalloc(plane)")) {
+        return nullptr;
+    }
+    if (!cuda_ok(cudaMemsetAsync(p, 0, bytes, g->st), "cudaMemsetAsync(plane)")) return nullptr;
+    g->planes.push_back(Plane{k, p});
+    g->version++;
+    return &g->planes.back();
+}
+
+void grid_zero(Grid *g)
+{
+    // timefield3d_zero_fields (timefield3d.c:108-121): fields, old fields,
+    // DFT accumulators and sources; plus the engine's CPML memory, monitors,
+    // probes and step counter
+    g->host_steps = 0;
+    if (!g->dev) return;
+    size_t es = esize(g);
+    for (int s = 0; s < 2; s++)
+        for (int m = 0; m < 6; m++) {
+            if (g->f[s][m]) cudaMemsetAsync(g->f[s][m], 0, (size_t)g->n * es, g->st);
+        }
+    for (int m = 0; m < 6; m++)
+        if (g->old[m]) cudaMemsetAsync(g->old[m], 0, (size_t)g->n * es, g->st);
+    size_t L2 = 2 * (size_t)g->L;
+    size_t sz[3] = {L2 * g->ny * g->nz * es, (size_t)g->nx * L2 * g->nz * es, (size_t)g->nx * g->ny * L2 * es};
+    for (int s = 0; s < 2; s++)
+        for (int a = 0; a < 3; a++)
+            for (int w = 0; w < 4; w++)
+                if (g->psi[s][a][w]) cudaMemsetAsync(g->psi[s][a][w], 0, sz[a], g->st);
+    for (auto &p : g->planes) g->plane_pool.push_back(p.p);
+    g->planes.clear();
+    if (g->d_dft_full) cudaMemsetAsync(g->d_dft_full, 0, (size_t)g->n * 6 * sizeof(double2), g->st);
+    for (auto &kv : g->d_dft_slice) cudaMemsetAsync(kv.second, 0, (size_t)g->nx * g->nz * 6 * sizeof(double2), g->st);
+    for (auto &mn : g->monitors) cudaMemsetAsync(mn.d_acc, 0, 2 * mn.nfreq * sizeof(double2), g->st);
+    if (g->d_probe_count) cudaMemsetAsync(g->d_probe_count, 0, g->probes.size() * sizeof(int), g->st);
+    cudaMemsetAsync(g->d_step, 0, sizeof(long long), g->st);
+    g->version++;
+    cuda_ok(cudaGetLastError(), "timefield3d_zero_fields");
+}
+
+// ---------------------------------------------------------------------------
+// the step
+// ---------------------------------------------------------------------------
+template <typename T> static bool step_split(Grid *g, double dt)
+{
+    GridView<T> v = view<T>(g, g->cur);
+    CpmlView<T> c = cpml_view<T>(g, g->cur);
+    SourcePlanes s = source_table(g);
+    const T tdt = (T)dt, div = (T)(1 / (g->dx)), tdx = (T)g->dx;
+    const bool cpml = g->boundary == FDTD_BOUNDARY_CPML;
+    if (g->boundary == FDTD_BOUNDARY_MUR) launch_save_shell<T>(v, g->st);
+    launch_update_E<T>(v, c, s, tdt, div, 1, g->nz - 1, g->sig_e, cpml, false, g->st);
+    if (g->boundary == FDTD_BOUNDARY_MUR) launch_mur<T>(v, tdt, tdx, 1, 0, g->nz, g->st);
+    launch_update_H<T>(v, c, s, tdt, div, 1, g->nz - 1, g->sig_m, g->mu_nonunit, cpml, false, g->st);
+    if (g->boundary == FDTD_BOUNDARY_MUR) launch_mur<T>(v, tdt, tdx, 0, 0, g->nz, g->st);
+    CKL("step");
+    return true;
+}
+
+static bool step_fused(Grid *g, double dt)
+{
+    FusedArgs a{};
+    a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
+    const int in = g->cur, out = 1 - g->cur;
+    for (int m = 0; m < 6; m++) { a.f_in[m] = (const float *)g->f[in][m]; a.f_out[m] = (float *)g->f[out][m]; }
+    for (int c = 0; c < 3; c++) { a.cb[c] = g->cb[c]; a.ca[c] = g->sig_e ? g->ca[c] : nullptr; }
+    a.hb = (float)(dt / g->dx);
+    a.dx = (float)g->dx;
+    a.L = g->boundary == FDTD_BOUNDARY_CPML ? g->L : 0;
+    for (int ax = 0; ax < 3; ax++) {
+        for (int w = 0; w < 4; w++) {
+            a.psi_in[ax][w] = (const float *)g->psi[in][ax][w];
+            a.psi_out[ax][w] = (float *)g->psi[out][ax][w];
+        }
+        for (int w = 0; w < 6; w++) a.prof[w][ax] = (const float *)g->prof[w][ax];
+    }
+    a.src = source_table(g);
+    launch_fused_step(a, g->st);
+    CKL("fused step");
+    g->cur = out;
+    return true;
+}
+
+bool enqueue_after_step(Grid *g, double dt)
+{
+    const void *const *fp = (const void *const *)g->d_fptr[g->cur];
+    const bool f64 = g->prec == FDTD_F64;
+    if (!g->probes.empty()) {
+        if (f64) launch_probes<double>((const double *const *)fp, g->d_probes, (int)g->probes.size(), g->d_probe_buf, g->probe_cap, g->d_probe_count, g->st);
+        else launch_probes<float>((const float *const *)fp, g->d_probes, (int)g->probes.size(), g->d_probe_buf, g->probe_cap, g->d_probe_count, g->st);
+    }
+    if (g->njobs > 0) {
+        double scale = (-0.5 * g->dx * g->dx);
+        if (f64) launch_overlap<double>((const double *const *)fp, g->nx, g->ny, g->d_jobs, g->njobs, g->d_partials, scale, dt, g->d_step, 0, g->st);
+        else launch_overlap<float>((const float *const *)fp, g->nx, g->ny, g->d_jobs, g->njobs, g->d_partials, scale, dt, g->d_step, 0, g->st);
+    }
+    for (auto &b : g->binds) {
+        TaperDev *td = nullptr;
+        adjoint3d_taper key{};
+        key.left = (int *)b.taper_key;
+        td = taper_lookup(key, false);
+        if (!td) continue;
+        if (!enqueue_taper_store(td, g, b.which, 0, g->d_step, b.t0, b.dir)) return false;
+    }
+    launch_step_advance(g->d_step, g->st);
+    CKL("after step");
+    return true;
+}
+
+bool rebuild_jobs(Grid *g)
+{
+    std::vector<OverlapJob> jobs;
+    for (auto &mn : g->monitors) {
+        auto it = priv_modes().find(mn.mode_key);
+        if (it == priv_modes().end()) continue;
+        OverlapJob j{};
+        j.cx = mn.cx; j.cy = mn.cy; j.cz = mn.cz;
+        j.mi = it->second.mi; j.mj = it->second.mj;
+        j.reverse = mn.reverse;
+        j.ratio = g->dx / it->second.disc;
+        j.mode = it->second.d;
+        j.inst = nullptr;
+        j.acc = mn.d_acc;
+        j.omega = mn.d_omega;
+        j.nfreq = mn.nfreq;
+        jobs.push_back(j);
+    }
+    g->njobs = (int)jobs.size();
+    if (g->njobs)
+        CK(cudaMemcpyAsync(g->d_jobs, jobs.data(), jobs.size() * sizeof(OverlapJob), cudaMemcpyHostToDevice, g->st));
+    g->version++;
+    return true;
+}
+
+bool enqueue_step(Grid *g, double dt, bool with_extras)
+{
+    if (g->sched.active) {
+        auto it = priv_modes().find(g->sched.mode_key);
+        Plane *pl = grid_plane(g, g->sched.cz, false);
+        if (it == priv_modes().end() || !pl) {
+            set_error(FDTD_ERR_ARG, "scheduled source not prepared");
+            return false;
+        }
+        const long long nxy = (long long)g->nx * g->ny, off = nxy * g->sched.cz;
+        const float *epp[3] = {g->ep[0] + off, g->ep[1] + off, g->ep[2] + off};
+        const float *mup[3] = {g->mu[0] + off, g->mu[1] + off, g->mu[2] + off};
+        launch_mode_source(pl->p, epp, mup, g->nx, g->ny, g->sched.cx, g->sched.cy, it->second.d, it->second.mi,
+                           it->second.mj, g->dx / it->second.disc, 0, 0, 0, g->sched.d_sched, g->d_step, g->sched.n,
+                           g->sched.reverse, g->sched.adjoint, g->st);
+    }
+    bool ok;
+    if (g->prec == FDTD_F64) ok = step_split<double>(g, dt);
+    else if (fused_path(g)) ok = step_fused(g, dt);
+    else ok = step_split<float>(g, dt);
+    if (!ok) return false;
+    return with_extras ? enqueue_after_step(g, dt) : true;
+}
+
+static bool prepare_run(Grid *g, double dt)
+{
+    if (!grid_prepare_step(g, dt)) return false;
+    if (!rebuild_jobs(g)) return false;
+    if (g->sched.active && !grid_plane(g, g->sched.cz, true)) return false;
+    for (auto &b : g->binds) {
+        adjoint3d_taper key{};
+        key.left = (int *)b.taper_key;
+        TaperDev *td = taper_lookup(key, false);
+        if (!td) {
+            set_error(FDTD_ERR_ARG, "bound taper no longer exists");
+            return false;
+        }
+        if (td->prec != g->prec || !td->d_cells) {
+            set_error(FDTD_ERR_ARG, "bound taper not prepared for this grid");
+            return false;
+        }
+    }
+    return true;
+}
+
+bool run_steps(Grid *g, double dt, int nsteps)
+{
+    if (nsteps <= 0) return true;
+    if (!prepare_run(g, dt)) return false;
+    const int G = 32;   // steps per captured graph (even: the fused path ping-pongs)
+    int full = nsteps / G, rest = nsteps % G;
+    if (full > 0) {
+        if (!g->graph || g->graph_steps != G || g->graph_dt != dt || g->graph_version != g->version ||
+            g->cur != 0) {
+            if (g->graph) {
+                cudaGraphExecDestroy(g->graph);
+                g->graph = nullptr;
+            }
+            int cur0 = g->cur;
+            cudaGraph_t gr;
+            CK(cudaStreamBeginCapture(g->st, cudaStreamCaptureModeThreadLocal));
+            bool ok = true;
+            for (int s = 0; s < G && ok; s++) ok = enqueue_step(g, dt, true);
+            cudaError_t ce = cudaStreamEndCapture(g->st, &gr);
+            if (!ok) {
+                if (ce == cudaSuccess) cudaGraphDestroy(gr);
+                g->cur = cur0;
+                return false;
+            }
+            CK(ce);
+            CK(cudaGraphInstantiate(&g->graph, gr, 0));
+            cudaGraphDestroy(gr);
+            g->graph_steps = G;
+            g->graph_dt = dt;
+            g->graph_version = g->version;
+            g->graph_cur = cur0;
+            if (g->cur != cur0) {
+                set_error(FDTD_ERR_CUDA, "internal: odd graph length");
+                return false;
+            }
+        }
+        for (int r = 0; r < full; r++) CK(cudaGraphLaunch(g->graph, g->st));
+    }
+    for (int s = 0; s < rest; s++)
+        if (!enqueue_step(g, dt, true)) return false;
+    g->host_steps += nsteps;
+    return true;
+}
+
+// ============================================================================
+// tapers
+// ============================================================================
+static std::unordered_map<const void *, TaperDev *> &taper_table()
+{
+    static std::unordered_map<const void *, TaperDev *> t;
+    return t;
+}
+
+TaperDev::~TaperDev()
+{
+    dfree(d_fwd);
+    dfree(d_adj);
+    dfree(d_cells);
+    dfree(d_grad);
+}
+
+TaperDev *taper_lookup(const adjoint3d_taper &t, bool create)
+{
+    auto &tab = taper_table();
+    auto it = tab.find(t.left);
+    if (it != tab.end()) return it->second;
+    if (!create) return nullptr;
+    TaperDev *td = new TaperDev();
+    td->key = t.left;
+    tab[t.left] = td;
+    return td;
+}
+
+void taper_unregister(const adjoint3d_taper &t)
+{
+    auto &tab = taper_table();
+    auto it = tab.find(t.left);
+    if (it == tab.end()) return;
+    cudaDeviceSynchronize();
+    delete it->second;
+    tab.erase(it);
+}
+
+bool taper_prepare(TaperDev *td, const adjoint3d_taper &t, Grid *g)
+{
+    if (!grid_ensure_device(g)) return false;
+    const int height = t.top - t.bottom, length = t.end - t.start;
+    if (height <= 0 || length <= 0 || t.duration <= 0 || t.seg_num <= 0) {
+        set_error(FDTD_ERR_ARG, "taper: empty storage box (height %d length %d duration %d seg_num %d)", height, length,
+                  t.duration, t.seg_num);
+        return false;
+    }
+    const int ncell = 2 * height * length;
+    const bool resize = td->ncell != ncell || td->duration != t.duration || td->prec != g->prec;
+    td->seg_num = t.seg_num; td->start = t.start; td->end = t.end; td->bottom = t.bottom; td->top = t.top;
+    td->height = height; td->length = length;
+    size_t es = g->prec == FDTD_F64 ? 8 : 4;
+    if (resize) {
+        cudaDeviceSynchronize();
+        dfree(td->d_fwd);
+        dfree(td->d_adj);
+        dfree(td->d_cells);
+        dfree(td->d_grad);
+        td->ncell = ncell;
+        td->duration = t.duration;
+        td->prec = g->prec;
+        td->edges_seen.clear();
+        size_t bytes = (size_t)t.duration * ncell * 3 * es;
+        if (!dalloc(&td->d_fwd, bytes, g->st) || !dalloc(&td->d_adj, bytes, g->st)) return false;
+        if (!dalloc(&td->d_cells, ncell * sizeof(long long), g->st, false)) return false;
+        if (!dalloc(&td->d_grad, ncell * sizeof(double), g->st)) return false;
+    }
+    std::vector<int> edges(t.left, t.left + t.seg_num + 1);
+    edges.insert(edges.end(), t.right, t.right + t.seg_num + 1);
+    if (edges != td->edges_seen || td->nx_seen != g->nx || td->ny_seen != g->ny) {
+        // edge pixel of (edge, j, k): adjoint3d.c:268-296, integer division
+        // inside round(), i.e. edge[n] + trunc(d (k - k0) / (k1 - k0))
+        std::vector<long long> cells(ncell);
+        for (int n = 0; n < t.seg_num; n++) {
+            int seg_mid = t.start + (n * length) / t.seg_num;
+            int seg_fwd = t.start + ((n + 1) * length) / t.seg_num;
+            for (int k = seg_mid; k < seg_fwd; k++)
+                for (int j = t.bottom; j < t.top; j++)
+                    for (int e = 0; e < 2; e++) {
+                        const int *edge = e == 0 ? t.right : t.left;
+                        int i = edge[n] + ((edge[n + 1] - edge[n]) * (k - seg_mid)) / (seg_fwd - seg_mid);
+                        if (i < 0 || i >= g->nx || j < 0 || j >= g->ny || k < 0 || k >= g->nz) {
+                            set_error(FDTD_ERR_ARG, "taper edge pixel (%d,%d,%d) outside the grid", i, j, k);
+                            return false;
+                        }
+                        cells[e + 2 * ((j - t.bottom) + (size_t)height * (k - t.start))] =
+                            i + (long long)g->nx * (j + (long long)g->ny * k);
+                    }
+        }
+        CK(cudaStreamSynchronize(g->st));
+        CK(cudaMemcpy(td->d_cells, cells.data(), ncell * sizeof(long long), cudaMemcpyHostToDevice));
+        td->edges_seen = edges;
+        td->nx_seen = g->nx;
+        td->ny_seen = g->ny;
+    }
+    return true;
+}
+
+bool enqueue_taper_store(TaperDev *td, Grid *g, int which, int t_index, const long long *d_step, int t0, int dir)
+{
+    const void *const *fp = (const void *const *)g->d_fptr[g->cur];
+    void *store = which ? td->d_adj : td->d_fwd;
+    if (g->prec == FDTD_F64)
+        launch_taper_store<double>((const double *const *)fp, td->d_cells, td->ncell, (double *)store, t_index, d_step, t0, dir, td->duration, g->st);
+    else
+        launch_taper_store<float>((const float *const *)fp, td->d_cells, td->ncell, (float *)store, t_index, d_step, t0, dir, td->duration, g->st);
+    CKL("taper store");
+    return true;
+}
+
+}  // namespace fdtd

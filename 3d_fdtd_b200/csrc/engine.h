@@ -1,0 +1,198 @@
+// engine.h -- device-side state of a grid and of a taper (internal header).
+//
+// A reference `timefield3d` is passed by value everywhere, so the engine keys
+// its device state on the struct's `fields` pointer (unique per grid, shared by
+// every by-value copy).  Tapers are keyed on their `left` pointer, modes on
+// `fields.m`.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/fdtd_b200.h"
+#include "kernels.h"
+
+namespace fdtd {
+
+// ---- status ----------------------------------------------------------------
+void set_error(int code, const char *fmt, ...);
+bool cuda_ok(cudaError_t e, const char *what);
+bool device_available();
+
+// ---- device modes ------------------------------------------------------------
+struct DevMode {
+    const void *key = nullptr;
+    uint64_t fingerprint = 0;
+    int mi = 0, mj = 0;
+    double disc = 0;
+    double2 *d = nullptr;
+};
+// registers (power-normalising the host mode on first sight) and returns the
+// device copy; null on failure
+DevMode *mode_device(const mode &m);
+void mode_release(const void *key);
+// host power normalisation, mode.c:1267-1379
+double mode_power_norm_host(const mode &m);
+void mode_power_normalize_host(const mode &m);
+// private power-normalised device copy of a mode (monitors, schedules), by handle
+const void *priv_mode_new(const mode &m);
+void priv_mode_free(const void *key);
+
+// ---- grid ------------------------------------------------------------------
+struct Plane {
+    int k;
+    float *p;
+};
+
+struct Monitor {
+    int cx, cy, cz, reverse, nfreq;
+    const void *mode_key;
+    double *d_omega = nullptr;
+    double2 *d_acc = nullptr;   // 2*nfreq: (sum, compensation)
+};
+
+struct ProbeRec {
+    ProbeJob job;
+    int cap;
+};
+
+struct Schedule {
+    bool active = false;
+    int cx, cy, cz, reverse, adjoint, n;
+    const void *mode_key = nullptr;
+    double *d_sched = nullptr;   // 3*n: amplitude, cos, sin
+};
+
+struct TaperBind {
+    const void *taper_key;
+    int which, t0, dir;
+};
+
+struct Grid {
+    timefield3d h{};          // host struct (pointers are the host mirrors)
+    int nx = 0, ny = 0, nz = 0;
+    long long n = 0;
+    double dx = 0;
+    int prec = FDTD_F64;
+    int boundary = FDTD_BOUNDARY_MUR;
+
+    // device state
+    bool dev = false;
+    cudaStream_t st = nullptr;
+    void *f[2][6] = {};       // field sets; set 1 is the ping-pong buffer of the fused path
+    int cur = 0;
+    void *old[6] = {};        // Mur snapshot
+    float *ep[3] = {}, *mu[3] = {}, *sig[6] = {};
+    bool sig_e = false, sig_m = false, mu_nonunit = false;
+    bool mat_dirty = true;
+    bool fields_from_host = false;   // host mirror must be uploaded before next use
+    void **d_fptr[2] = {};           // device arrays of the 6 field pointers per set
+
+    // CPML
+    int L = 0, order = 3;
+    double smax = -1, kmax = 1, amax = 0;
+    double prof_dt = 0;
+    void *psi[2][3][4] = {};
+    void *prof[6][3] = {};
+
+    // FP32 fused-path coefficients
+    float *cb[3] = {}, *ca[3] = {};
+    double coef_dt = 0;
+    bool coef_valid = false;
+
+    // sources
+    std::vector<Plane> planes;
+    std::vector<float *> plane_pool;
+
+    // step counter, overlap scratch
+    long long *d_step = nullptr;
+    long long host_steps = 0;
+    OverlapJob *d_jobs = nullptr;       // monitors
+    int jobs_cap = 0, njobs = 0;
+    OverlapJob *d_job1 = nullptr;       // single compat overlap
+    double2 *d_partials = nullptr;
+    double2 *d_inst = nullptr;
+    double2 *h_inst = nullptr;          // pinned
+    std::vector<Monitor> monitors;
+
+    // probes
+    std::vector<ProbeRec> probes;
+    ProbeJob *d_probes = nullptr;
+    double *d_probe_buf = nullptr;
+    int *d_probe_count = nullptr;
+    int probe_cap = 0;
+
+    // running DFTs: whole grid, and y-slices by index
+    double2 *d_dft_full = nullptr;
+    std::map<int, double2 *> d_dft_slice;
+
+    // scheduled source, taper binds
+    Schedule sched;
+    std::vector<TaperBind> binds;
+
+    // staging
+    double *d_aos = nullptr;            // 6n doubles, for host mirror transfers
+    int *d_flag = nullptr;              // 12 material flags
+    int *h_flag = nullptr;              // pinned
+
+    // captured step graphs
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    double graph_dt = 0;
+    uint64_t graph_version = 0;
+    int graph_cur = 0;
+    uint64_t version = 1;               // bumped on any configuration change
+
+    ~Grid();
+};
+
+Grid *grid_lookup(const timefield3d &psi, bool quiet = false);
+Grid *grid_register(const timefield3d &psi);
+void grid_unregister(const timefield3d &psi);
+
+// device lifetime
+bool grid_ensure_device(Grid *g);              // allocate device arrays, upload what is dirty
+bool grid_upload_materials(Grid *g);
+bool grid_upload_fields(Grid *g);              // host mirror -> device
+bool grid_download_fields(Grid *g);            // device -> host mirror (waits)
+bool grid_set_precision(Grid *g, int prec);
+bool grid_prepare_step(Grid *g, double dt);    // profiles / coefficients for dt
+Plane *grid_plane(Grid *g, int k, bool create);
+void grid_zero(Grid *g);
+
+// queued work
+bool enqueue_step(Grid *g, double dt, bool with_extras);
+bool enqueue_after_step(Grid *g, double dt);
+bool run_steps(Grid *g, double dt, int nsteps);
+bool rebuild_jobs(Grid *g);
+
+// typed helpers
+template <typename T> GridView<T> view(Grid *g, int set);
+template <typename T> CpmlView<T> cpml_view(Grid *g, int in_set);
+SourcePlanes source_table(Grid *g);
+
+// taper
+struct TaperDev {
+    const void *key = nullptr;
+    int seg_num = 0, start = 0, end = 0, bottom = 0, top = 0, duration = 0;
+    int height = 0, length = 0, ncell = 0;
+    int prec = -1;
+    void *d_fwd = nullptr, *d_adj = nullptr;
+    long long *d_cells = nullptr;
+    std::vector<int> edges_seen;   // left/right copy the cell list was built for
+    int nx_seen = 0, ny_seen = 0;
+    double *d_grad = nullptr;
+    ~TaperDev();
+};
+TaperDev *taper_lookup(const adjoint3d_taper &t, bool create);
+void taper_unregister(const adjoint3d_taper &t);
+bool taper_prepare(TaperDev *td, const adjoint3d_taper &t, Grid *g);
+bool enqueue_taper_store(TaperDev *td, Grid *g, int which, int t_index, const long long *d_step, int t0, int dir);
+
+std::mutex &api_mutex();
+
+}  // namespace fdtd

@@ -1,0 +1,81 @@
+// kernels.h -- host-side launchers of the device kernels (internal header).
+#pragma once
+
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace fdtd {
+
+// one overlap reduction: plane cz of the grid against a device mode
+struct OverlapJob {
+    int cx, cy, cz;
+    int mi, mj;
+    int reverse;
+    double ratio;           // grid disc / mode disc
+    const double2 *mode;    // 6*mi*mj complex, entry 6*(i + mi*j) + m
+    double2 *inst;          // instantaneous overlap out (or null)
+    double2 *acc;           // per-frequency (sum, compensation) pairs (or null)
+    const double *omega;    // n_freq angular frequencies
+    int nfreq;
+};
+
+struct ProbeJob {
+    long long q;
+    int m;
+};
+
+// yee_split.cu
+template <typename T>
+void launch_update_E(const GridView<T> &g, const CpmlView<T> &c, const SourcePlanes &s, T dt, T divisor, int k_lo,
+                     int k_hi, bool sig, bool cpml, bool expl, cudaStream_t st);
+template <typename T>
+void launch_update_H(const GridView<T> &g, const CpmlView<T> &c, const SourcePlanes &s, T dt, T divisor, int k_lo,
+                     int k_hi, bool sig, bool mu, bool cpml, bool expl, cudaStream_t st);
+template <typename T> void launch_save_shell(const GridView<T> &g, cudaStream_t st);
+template <typename T> void launch_mur(const GridView<T> &g, T dt, T dx, int efield, int ks, int ke, cudaStream_t st);
+template <typename T> void launch_aos_to_soa(const double *aos, T *const d[6], long long n, cudaStream_t st);
+template <typename T> void launch_soa_to_aos(double *aos, T *const s[6], long long n, cudaStream_t st);
+
+// yee_fused.cu (FP32 single-pass E+H step)
+struct FusedArgs {
+    int nx, ny, nz;
+    const float *f_in[6];
+    float *f_out[6];
+    const float *cb[3];      // E curl coefficients, per component (main_coeff / dx)
+    const float *ca[3];      // E self coefficients (null: lossless, ca = 1)
+    float hb;                // H curl coefficient (dt / (mu dx)), uniform mu = 1, no magnetic loss
+    float dx;
+    int L;                   // CPML thickness (0: none)
+    const float *psi_in[3][4];
+    float *psi_out[3][4];
+    const float *prof[6][3];
+    SourcePlanes src;
+};
+int fused_supported(int nx, int ny, int nz);
+void launch_fused_step(const FusedArgs &a, cudaStream_t st);
+
+// aux_kernels.cu
+void launch_mode_source(float *plane, const float *const ep_plane[3], const float *const mu_plane[3], int nx, int ny,
+                        int cx, int cy, const double2 *mode, int mi, int mj, double ratio, double amplitude,
+                        double cph, double sph, const double *sched, const long long *step, int nsched, int reverse,
+                        int adjoint, cudaStream_t st);
+void launch_set_value(float *p, long long idx, float v, cudaStream_t st);
+int overlap_parts(int nx, int ny);
+template <typename T>
+void launch_overlap(const T *const *f_dev, int nx, int ny, const OverlapJob *jobs_dev, int njobs, double2 *partials,
+                    double scale, double dt, const long long *step, int step_offset, cudaStream_t st);
+template <typename T>
+void launch_dft(const T *const *f_dev, int nx, int ny, int nz, int slice, int k_lo, int k_hi, double tr, double ti,
+                double2 *acc, cudaStream_t st);
+template <typename T>
+void launch_probes(const T *const *f_dev, const ProbeJob *probes, int np, double *buf, int cap, int *count,
+                   cudaStream_t st);
+void launch_step_advance(long long *step, cudaStream_t st);
+template <typename T>
+void launch_taper_store(const T *const *f_dev, const long long *cells, int ncell, T *store, int t_index,
+                        const long long *step, int t0, int dir, int duration, cudaStream_t st);
+template <typename T>
+void launch_ep_gradient(const T *fwd, const T *adj, int ncell, int duration, double *grad, cudaStream_t st);
+void launch_check_finite(const float *a, long long n, int *bad, cudaStream_t st);
+
+}  // namespace fdtd

@@ -1,0 +1,293 @@
+/*
+ * fdtd_b200.h -- C ABI of libfdtd_b200.so, the B200 engine for the FDTD hot path
+ * of QJohn2017/3D_FDTD.
+ *
+ * Drop-in: the library exports the reference's own FDTD (timefield3d.h) and taper
+ * adjoint (adjoint3d.h) entry points with the same names, by-value struct
+ * arguments and meaning, so a program written against the reference links
+ * against this library instead of timefield3d.o and adjoint3d.o and keeps the
+ * reference's complex.o, matrix.o and mode.o.  The struct layouts below are
+ * identical to the reference's (timefield3d.h:15-27, mode.h:13-22,
+ * matrix.h:11-16, complex.h:11-15, adjoint3d.h:37-58).  If a translation unit
+ * also includes the reference's headers, include those first: the type blocks
+ * here are skipped when the reference's include guards are already defined.
+ *
+ * What changes behind the same calls:
+ *   - field state lives on the GPU; psi.fields is a host mirror refreshed by
+ *     timefield3d_get_fields, timefield3d_get_edge_fields and
+ *     timefield3d_sync_host;
+ *   - materials stay host-authoritative: the timefield3d_set_* rasterisers write
+ *     psi.ep/mu/sig on the host exactly as the reference does, and the next
+ *     device operation uploads them;
+ *   - calls queue GPU work on the grid's own stream and return; only calls
+ *     that return data to the host wait for it;
+ *   - errors never abort: every entry point records a status, read with
+ *     fdtd_last_error().  There is no CPU fallback: without a usable GPU the
+ *     device entry points fail with FDTD_ERR_NO_DEVICE and print why.
+ *
+ * Extensions (no reference counterpart) are grouped at the end: precision
+ * (the reference's FP64 or FP32 fields), CPML boundary, point sources, probes,
+ * multi-wavelength overlap monitors, a scheduled mode source and a captured
+ * multi-step run.
+ */
+#ifndef FDTD_B200_H
+#define FDTD_B200_H
+
+#include <stdio.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- reference-compatible types (layouts identical to the reference) ---- */
+#ifndef _complex_h
+struct complex_ { double re, im; };                       /* complex.h:11-15 */
+typedef struct complex_ complex;
+#endif
+#ifndef _matrix_h
+struct matrix_ { int i, j; complex *m; };                 /* matrix.h:11-16 */
+typedef struct matrix_ matrix;
+#endif
+#ifndef _mode_h
+struct mode_ { int i, j; double disc; matrix pml; matrix ep; matrix mu; matrix fields; }; /* mode.h:13-22 */
+typedef struct mode_ mode;
+#endif
+#ifndef _timefield3d_h
+struct timefield3d_ {                                     /* timefield3d.h:15-27 */
+    int i, j, k;
+    double disc;
+    float *ep;
+    float *mu;
+    float *sig;
+    double *fields;
+    double *old_fields;
+    complex *fourier_fields;
+    float *sources;
+};
+typedef struct timefield3d_ timefield3d;
+#endif
+#ifndef _adjoint3d_h
+struct adjoint3d_taper_ {                                 /* adjoint3d.h:37-58 */
+    double ep;
+    double mu;
+    int seg_num;
+    int start;
+    int end;
+    int bottom;
+    int top;
+    int duration;
+    int *left;
+    int *right;
+    double *forward_fields;
+    double *adjoint_fields;
+    double *ep_gradient;
+    double *left_grad;
+    double *right_grad;
+};
+typedef struct adjoint3d_taper_ adjoint3d_taper;
+#endif
+
+/* =========================================================================
+ * Reference entry points (timefield3d.h).  Each replaces the reference
+ * function of the same name; the cited line is its declaration.
+ * ========================================================================= */
+
+/* timefield3d.h:30 -- allocates host mirrors; the device grid is created on first use */
+timefield3d timefield3d_new(int i, int j, int k, double disc);
+/* timefield3d.h:31 */
+void timefield3d_free(timefield3d psi);
+/* timefield3d.h:32 -- copies materials and current fields into a new grid */
+timefield3d timefield3d_copy(timefield3d psi);
+/* timefield3d.h:33 -- zeroes fields, boundary memory, sources, running DFTs, monitors */
+void timefield3d_zero_fields(timefield3d psi);
+/* timefield3d.h:34 -- waits for the grid, returns a malloc'd AoS double copy */
+double *timefield3d_get_fields(timefield3d psi);
+/* timefield3d.h:35 -- same, only the 2-cell shell filled (other entries unspecified) */
+double *timefield3d_get_edge_fields(timefield3d psi);
+/* timefield3d.h:36 -- snapshot of the 2-cell shell used by the Mur boundary */
+void timefield3d_update_old_edge_fields(timefield3d psi);
+
+/* timefield3d.h:39-53 -- gnuplot plots in the reference.  No graphics here: each
+ * call writes the slice as raw float64 (header: int n1, int n2) to
+ * $FDTD_PLOT_DIR/<name>_<index>.bin when FDTD_PLOT_DIR is set, else does nothing. */
+void timefield3d_plot_Ex_x_slice(timefield3d psi, int slice_index);
+void timefield3d_plot_Ex_y_slice(timefield3d psi, int slice_index);
+void timefield3d_plot_Ex_z_slice(timefield3d psi, int slice_index);
+void timefield3d_plot_Ey_x_slice(timefield3d psi, int slice_index);
+void timefield3d_plot_Ey_y_slice(timefield3d psi, int slice_index);
+void timefield3d_plot_Ey_z_slice(timefield3d psi, int slice_index);
+void timefield3d_plot_Ez_x_slice(timefield3d psi, int slice_index);
+void timefield3d_plot_Ez_y_slice(timefield3d psi, int slice_index);
+void timefield3d_plot_Ez_z_slice(timefield3d psi, int slice_index);
+void timefield3d_plot_Ex_x_slice_fourier(timefield3d psi, int slice_index);
+void timefield3d_plot_Ex_y_slice_fourier(timefield3d psi, int slice_index);
+void timefield3d_plot_Ex_z_slice_fourier(timefield3d psi, int slice_index);
+void timefield3d_plot_permittivity_x_slice(timefield3d psi, int slice_index);
+void timefield3d_plot_permittivity_y_slice(timefield3d psi, int slice_index);
+void timefield3d_plot_permittivity_z_slice(timefield3d psi, int slice_index);
+
+/* timefield3d.h:56-70 -- material rasterisers; host arrays, uploaded on next device use */
+void timefield3d_set_background(timefield3d psi, float ep, float mu);
+void timefield3d_set_top_half_plane(timefield3d psi, float ep, float mu, int bottom);
+void timefield3d_set_background_permittivity(timefield3d psi, float ep);
+void timefield3d_set_background_permeability(timefield3d psi, float mu);
+void timefield3d_set_background_electric_conductivity(timefield3d psi, float sig);
+void timefield3d_set_background_magnetic_conductivity(timefield3d psi, float sig);
+void timefield3d_set_background_complex_permittivity(timefield3d psi, double omega, float real_ep, float imag_ep);
+void timefield3d_set_prism_permittivity(timefield3d psi, float ep, int start_x, int end_x, int start_y, int end_y, int start_z, int end_z);
+void timefield3d_set_prism_electric_conductivity(timefield3d psi, float sig, int start_x, int end_x, int start_y, int end_y, int start_z, int end_z);
+void timefield3d_set_prism_complex_permittivity(timefield3d psi, double omega, float real_ep, float imag_ep, int start_x, int end_x, int start_y, int end_y, int start_z, int end_z);
+void timefield3d_set_waveguide(timefield3d psi, float ep, int start_x, int end_x, int start_z, int end_z, int bottom, int top);
+void timefield3d_set_taper(timefield3d psi, double ep, double mu, int start_left, int start_right, int end_left, int end_right, int start_z, int end_z, int bottom, int top);
+
+/* timefield3d.h:73-76 -- explicit (non-semi-implicit) interior updates, whole grid */
+void timefield3d_apply_H_timestep(timefield3d psi, double delta_t);
+void timefield3d_apply_E_timestep(timefield3d psi, double delta_t);
+/* timefield3d.h:75-76 -- semi-implicit interior update of z in [start+1, stop-1) */
+void timefield3d_apply_H_timestep_zsection(timefield3d psi, double delta_t, int start_index, int stop_index);
+void timefield3d_apply_E_timestep_zsection(timefield3d psi, double delta_t, int start_index, int stop_index);
+/* timefield3d.h:77-80 -- Mur boundary; old_field is an AoS shell copy from
+ * timefield3d_get_edge_fields (host).  The zsection forms use psi.old_fields,
+ * i.e. the snapshot taken by timefield3d_update_old_edge_fields. */
+void timefield3d_apply_H_first_order_abc(timefield3d psi, double *old_field, double delta_t);
+void timefield3d_apply_E_first_order_abc(timefield3d psi, double *old_field, double delta_t);
+void timefield3d_apply_H_first_order_abc_zsection(timefield3d psi, double delta_t, int start_index, int stop_index);
+void timefield3d_apply_E_first_order_abc_zsection(timefield3d psi, double delta_t, int start_index, int stop_index);
+/* timefield3d.h:81 -- explicit-update step: shell copy, E, E-ABC, H, H-ABC */
+void timefield3d_apply_timestep(timefield3d psi, double delta_t);
+/* timefield3d.h:82-83 -- the semi-implicit step the reference driver uses
+ * (timefield3d.c:2787-2849).  With the CPML extension enabled the Mur passes
+ * are replaced by the CPML terms inside the update. */
+void timefield3d_apply_timestep_omp(timefield3d psi, double delta_t);
+void timefield3d_apply_timestep_omp_full(timefield3d psi, double delta_t);
+/* timefield3d.h:84-89 -- running single-frequency DFT, on device (complex double) */
+void timefield3d_update_fourier_fields(timefield3d psi, double phase);
+void timefield3d_update_fourier_fields_y_slice(timefield3d psi, double phase, int slice_index);
+void timefield3d_update_fourier_fields_zsection(timefield3d psi, double phase, int start_index, int stop_index);
+void timefield3d_update_fourier_fields_y_slice_zsection(timefield3d psi, double phase, int slice_index, int start_index, int stop_index);
+void timefield3d_update_fourier_fields_omp(timefield3d psi, double phase);
+void timefield3d_update_fourier_fields_y_slice_omp(timefield3d psi, double phase, int slice_index);
+
+/* timefield3d.h:95-96 -- mode plane sources.  The mode is power-normalised in
+ * place on first use (as the reference does on every call) and kept on the
+ * device; see timefield3d_release_mode. */
+void timefield3d_mode_source(timefield3d psi, int center_x, int center_y, int center_z, mode source_mode, double phase, double amplitude, int reverse);
+void timefield3d_mode_source_adjoint(timefield3d psi, int center_x, int center_y, int center_z, mode source_mode, double phase, int reverse);
+/* timefield3d.h:97-98 -- Gaussian-beam sources: not provided (FDTD_ERR_UNSUPPORTED) */
+void timefield3d_TE_gaussian_source(timefield3d psi, int center_x, int center_y, int center_z, double width, double omega, double phase, double amplitude);
+void timefield3d_TM_gaussian_source(timefield3d psi, int center_x, int center_y, int center_z, double width, double omega, double phase, double amplitude);
+/* timefield3d.h:101 -- instantaneous mode overlap on plane z; adds e^{i phase} x
+ * overlap to *cumulative_overlap.  Waits for the grid (it returns a value). */
+complex timefield3d_mode_overlap(timefield3d psi, int center_x, int center_y, int center_z, mode overlap_mode, double phase, int reverse, complex *cumulative_overlap);
+/* timefield3d.h:104 -- binarised permittivity slice writer (host) */
+void timefield3d_file_write_permittivity_y_slice(timefield3d psi, char *filename, int left, int right, int start, int end, int y_slice, double ep_min, double ep_max);
+
+/* =========================================================================
+ * Reference entry points (adjoint3d.h, taper part).  Edge-field storage lives
+ * on the device (E components only, the precision of the grid); the host
+ * arrays forward_fields/adjoint_fields are filled only by
+ * adjoint3d_taper_sync_host.
+ * ========================================================================= */
+/* adjoint3d.h:60 */
+adjoint3d_taper adjoint3d_taper_new(double ep, double mu, int seg_num, int start, int end, int *left, int *right, int bottom, int top, int duration);
+/* adjoint3d.h:61 (host raster, adjoint3d.c:243-257) */
+void adjoint3d_taper_insert(timefield3d psi, adjoint3d_taper taper);
+/* adjoint3d.h:62-63 -- gather E on the rasterised edge pixels at time index timestep */
+void adjoint3d_taper_store_forward_fields(adjoint3d_taper taper, timefield3d main_fields, int timestep);
+void adjoint3d_taper_store_adjoint_fields(adjoint3d_taper taper, timefield3d main_fields, int timestep);
+/* adjoint3d.h:64 -- sum_t sum_{m<3} E_fwd E_adj on the device in FP64; fills taper.ep_gradient */
+void adjoint3d_taper_calculate_ep_gradient(adjoint3d_taper taper);
+/* adjoint3d.h:65 -- hat-weighted vertex gradients (host, from taper.ep_gradient) */
+void adjoint3d_taper_calculate_gradients_from_ep_gradient(adjoint3d_taper taper, double ep_diff);
+/* adjoint3d.h:68-69 -- integer-pixel edge updates (host) */
+int adjoint3d_taper_update_symmetric(adjoint3d_taper taper, double improvement_goal, double disc, int min_width);
+int adjoint3d_taper_update_asymmetric(adjoint3d_taper taper, double improvement_goal, double disc, int min_width);
+/* adjoint3d.c:42 defines the reference's release function as adjointd3d_free (its
+ * header says adjoint3d_free); this library releases tapers with: */
+void adjoint3d_taper_free(adjoint3d_taper taper);
+
+/* =========================================================================
+ * Extensions (no reference counterpart)
+ * ========================================================================= */
+enum fdtd_status {
+    FDTD_OK = 0,
+    FDTD_ERR_NO_DEVICE = 1,     /* no CUDA device or driver */
+    FDTD_ERR_CUDA = 2,          /* a CUDA call failed */
+    FDTD_ERR_ARG = 3,           /* invalid argument or unknown grid */
+    FDTD_ERR_ALLOC = 4,         /* host or device allocation failed */
+    FDTD_ERR_UNSUPPORTED = 5,   /* entry point or combination not provided */
+    FDTD_ERR_TIMEOUT = 6,       /* a bounded device wait gave up */
+    FDTD_ERR_NONFINITE = 7      /* NaN/Inf found in materials */
+};
+enum fdtd_precision { FDTD_F64 = 0, FDTD_F32 = 1 };
+enum fdtd_boundary { FDTD_BOUNDARY_MUR = 0, FDTD_BOUNDARY_CPML = 1, FDTD_BOUNDARY_PEC = 2 };
+
+/* status of the last failing call on this thread (sticky until cleared) */
+int fdtd_last_error(void);
+const char *fdtd_last_error_message(void);
+const char *fdtd_error_string(int code);
+void fdtd_clear_error(void);
+int fdtd_device_count(void);
+const char *fdtd_version(void);
+
+/* Grid configuration.  Precision FDTD_F64 (default) reproduces the reference's
+ * double fields; FDTD_F32 keeps fields and update coefficients in float.
+ * Changing precision or boundary keeps the current fields. */
+int timefield3d_set_precision(timefield3d psi, int precision);
+int timefield3d_set_boundary(timefield3d psi, int boundary);
+/* CPML of `thickness` cells on every face, polynomial grading `order`;
+ * sigma_max <= 0 selects 0.8 (order+1)/disc; kappa_max >= 1; alpha_max >= 0.
+ * Profiles depend on delta_t and are rebuilt when the step size changes.
+ * Implies timefield3d_set_boundary(psi, FDTD_BOUNDARY_CPML). */
+int timefield3d_set_cpml(timefield3d psi, int thickness, int order, double sigma_max, double kappa_max, double alpha_max);
+
+/* host mirror <-> device */
+int timefield3d_sync_host(timefield3d psi);       /* device fields -> psi.fields (waits) */
+int timefield3d_sync_device(timefield3d psi);     /* psi.fields, ep, mu, sig, sources -> device */
+int timefield3d_synchronize(timefield3d psi);     /* waits for all queued work */
+/* one source sample, without touching the rest of the sources (component m = 0..5) */
+int timefield3d_set_source_value(timefield3d psi, int i, int j, int k, int m, float value);
+/* one field value (waits) */
+double timefield3d_get_field_value(timefield3d psi, int i, int j, int k, int m);
+
+/* Probes: after every step, component m at (i,j,k) is appended on the device.
+ * read copies the first `count` samples of probe `id` into out (waits). */
+int timefield3d_add_probe(timefield3d psi, int i, int j, int k, int m, int capacity);
+int timefield3d_read_probe(timefield3d psi, int id, double *out, int count);
+int timefield3d_clear_probes(timefield3d psi);
+
+/* Mode-overlap monitors: after every step n (0-based count of steps already
+ * taken when the step started) the instantaneous overlap of
+ * timefield3d_mode_overlap is formed on the device and accumulated as
+ * O_l += e^{i omega_l n delta_t} o(n), in FP64 with compensated summation, for
+ * each of n_freq angular frequencies.  Returns the monitor id (>= 0) or -1. */
+int timefield3d_add_overlap_monitor(timefield3d psi, int center_x, int center_y, int center_z, mode overlap_mode, int reverse, int n_freq, const double *omega);
+int timefield3d_read_overlap_monitor(timefield3d psi, int id, complex *out);   /* n_freq values (waits) */
+int timefield3d_clear_monitors(timefield3d psi);
+/* number of completed steps since the last timefield3d_zero_fields */
+long long timefield3d_step_count(timefield3d psi);
+
+/* Scheduled mode source: before step n the plane source of
+ * timefield3d_mode_source (adjoint = 0) or timefield3d_mode_source_adjoint
+ * (adjoint = 1) is written with amplitude[n] and phase[n], n < nsteps.
+ * Applied by timefield3d_run. */
+int timefield3d_set_source_schedule(timefield3d psi, int center_x, int center_y, int center_z, mode source_mode, int reverse, int adjoint, int nsteps, const double *amplitude, const double *phase);
+int timefield3d_clear_source_schedule(timefield3d psi);
+/* Bind a taper's edge store to timefield3d_run: after step n the edge fields
+ * are stored at time index t0 + dir*n (which = 0 forward, 1 adjoint). */
+int adjoint3d_taper_bind_store(adjoint3d_taper taper, timefield3d psi, int which, int t0, int dir);
+int adjoint3d_taper_unbind_store(adjoint3d_taper taper, timefield3d psi);
+/* nsteps x (scheduled source, timefield3d_apply_timestep_omp_full, probes,
+ * monitors, bound taper stores), captured in CUDA graphs; returns at once. */
+int timefield3d_run(timefield3d psi, double delta_t, int nsteps);
+
+/* forget the device copy of a mode (call after editing mode.fields in place) */
+int timefield3d_release_mode(mode m);
+/* copy the device edge storage into taper.forward_fields/adjoint_fields in the
+ * reference layout [t][k][j][edge][6] (E components; H left zero) */
+int adjoint3d_taper_sync_host(adjoint3d_taper taper);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FDTD_B200_H */

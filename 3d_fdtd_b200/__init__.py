@@ -149,6 +149,12 @@ SIGNATURES = {
     "timefield3d_run": (i, [T, d, i]),
     "timefield3d_release_mode": (i, [M]),
     "adjoint3d_taper_sync_host": (i, [P]),
+    "fdtd_set_device": (i, [i]),
+    "fdtd_launch_count": (ll, []),
+    "timefield3d_get_stream": (C.c_void_p, [T]),
+    "timefield3d_upload_materials": (i, [T]),
+    "timefield3d_set_kernel_timing": (i, [T, i]),
+    "timefield3d_read_kernel_timing": (i, [T, dp, C.POINTER(ll)]),
 }
 
 
@@ -208,6 +214,10 @@ class HostMode:
         self.struct = Mode(mi, mj, self.disc, Matrix(2 * mi * mj, 1, cptr(self.pml)),
                            Matrix(3 * mi * mj, 1, cptr(self.ep)), Matrix(3 * mi * mj, 1, cptr(self.mu)),
                            Matrix(6 * mi * mj, 1, cptr(self.fields)))
+        # the library writes through these pointers (power normalisation in
+        # place, as the reference does): the struct keeps its arrays alive even
+        # when only `HostMode(...).struct` is held
+        self.struct._owner = self
 
     @property
     def mi(self):

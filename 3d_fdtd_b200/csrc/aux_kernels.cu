@@ -279,12 +279,17 @@ void launch_mode_source(float *plane, const float *const ep_plane[3], const floa
     long long nxy = (long long)nx * ny;
     int blocks = (int)((nxy + 255) / 256);
     if (blocks > 1184) blocks = 1184;
+    note_launch();
     k_mode_source<<<blocks, 256, 0, st>>>(plane, ep_plane[0], ep_plane[1], ep_plane[2], mu_plane[0], mu_plane[1],
                                           mu_plane[2], nx, ny, cx, cy, mode, mi, mj, ratio, amplitude, cph, sph, sched,
                                           step, nsched, reverse, adjoint);
 }
 
-void launch_set_value(float *p, long long idx, float v, cudaStream_t st) { k_set_value<<<1, 1, 0, st>>>(p, idx, v); }
+void launch_set_value(float *p, long long idx, float v, cudaStream_t st)
+{
+    note_launch();
+    k_set_value<<<1, 1, 0, st>>>(p, idx, v);
+}
 
 int overlap_parts(int nx, int ny)
 {
@@ -299,7 +304,9 @@ void launch_overlap(const T *const *f_dev, int nx, int ny, const OverlapJob *job
 {
     if (njobs <= 0) return;
     int parts = overlap_parts(nx, ny);
+    note_launch();
     k_overlap_partial<T><<<dim3(parts, njobs), 256, 0, st>>>(f_dev, nx, ny, jobs_dev, partials, parts);
+    note_launch();
     k_overlap_finalize<<<njobs, 32, 0, st>>>(jobs_dev, njobs, partials, parts, scale, dt, step, step_offset);
 }
 
@@ -311,6 +318,7 @@ void launch_dft(const T *const *f_dev, int nx, int ny, int nz, int slice, int k_
     long long cnt = slice >= 0 ? (long long)nx * (k_hi - k_lo) : (long long)nx * ny * (k_hi - k_lo);
     int blocks = (int)((cnt + 255) / 256);
     if (blocks > 4736) blocks = 4736;
+    note_launch();
     k_dft<T><<<blocks, 256, 0, st>>>(f_dev, nx, ny, nz, slice, k_lo, k_hi, tr, ti, acc);
 }
 
@@ -319,10 +327,15 @@ void launch_probes(const T *const *f_dev, const ProbeJob *probes, int np, double
                    cudaStream_t st)
 {
     if (np <= 0) return;
+    note_launch();
     k_probes<T><<<(np + 127) / 128, 128, 0, st>>>(f_dev, probes, np, buf, cap, count);
 }
 
-void launch_step_advance(long long *step, cudaStream_t st) { k_step_advance<<<1, 1, 0, st>>>(step); }
+void launch_step_advance(long long *step, cudaStream_t st)
+{
+    note_launch();
+    k_step_advance<<<1, 1, 0, st>>>(step);
+}
 
 template <typename T>
 void launch_taper_store(const T *const *f_dev, const long long *cells, int ncell, T *store, int t_index,
@@ -331,6 +344,7 @@ void launch_taper_store(const T *const *f_dev, const long long *cells, int ncell
     if (ncell <= 0) return;
     int blocks = (ncell + 255) / 256;
     if (blocks > 592) blocks = 592;
+    note_launch();
     k_taper_store<T><<<blocks, 256, 0, st>>>(f_dev, cells, ncell, store, t_index, step, t0, dir, duration);
 }
 
@@ -338,6 +352,7 @@ template <typename T>
 void launch_ep_gradient(const T *fwd, const T *adj, int ncell, int duration, double *grad, cudaStream_t st)
 {
     if (ncell <= 0) return;
+    note_launch();
     k_ep_gradient<T><<<(ncell + 127) / 128, 128, 0, st>>>(fwd, adj, ncell, duration, grad);
 }
 
@@ -345,7 +360,10 @@ void launch_check_finite(const float *a, long long n, int *bad, cudaStream_t st)
 {
     int blocks = (int)((n + 255) / 256);
     if (blocks > 2368) blocks = 2368;
-    if (blocks > 0) k_check_finite<<<blocks, 256, 0, st>>>(a, n, bad);
+    if (blocks > 0) {
+        note_launch();
+        k_check_finite<<<blocks, 256, 0, st>>>(a, n, bad);
+    }
 }
 
 #define FDTD_INST(T)                                                                                               \

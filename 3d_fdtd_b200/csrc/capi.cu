@@ -28,11 +28,11 @@ Grid *dev_grid(const timefield3d &psi)
     return g;
 }
 
-void mark_materials(const timefield3d &psi)
+void mark_materials(const timefield3d &psi, int mask)
 {
     Grid *g = grid_lookup(psi, true);
     if (g) {
-        g->mat_dirty = true;
+        g->mat_dirty |= mask;
         g->version++;
     }
 }
@@ -140,6 +140,7 @@ bool sync_fourier_host(Grid *g)
 {
     if (!g->dev || (!g->d_dft_full && g->d_dft_slice.empty())) return true;
     complex *h = g->h.fourier_fields;
+    g->host_mirror_written = true;
     const long long n = g->n;
     if (!cuda_ok(cudaStreamSynchronize(g->st), "sync")) return false;
     if (g->d_dft_full) {
@@ -312,20 +313,15 @@ void timefield3d_zero_fields(timefield3d psi)
     // engine's mirrors are only meaningful after a sync, so clear only what a
     // sync may have written
     size_t n = (size_t)psi.i * psi.j * psi.k;
-    if (g->dev) {
-        memset(psi.fields, 0, 6 * n * sizeof(double));
-        if (g->d_dft_full) memset(psi.fourier_fields, 0, 6 * n * sizeof(complex));
-        else
-            for (auto &kv : g->d_dft_slice)
-                for (int k = 0; k < psi.k; k++)
-                    for (int i = 0; i < psi.i; i++)
-                        memset(&psi.fourier_fields[6 * (i + (size_t)psi.i * (kv.first + (size_t)psi.j * k))], 0,
-                               6 * sizeof(complex));
-    } else {
+    if (!g->dev || g->host_mirror_written) {
         memset(psi.fields, 0, 6 * n * sizeof(double));
         memset(psi.old_fields, 0, 6 * n * sizeof(double));
-        memset(psi.sources, 0, 6 * n * sizeof(float));
+        memset(psi.fourier_fields, 0, 6 * n * sizeof(complex));
     }
+    if (!g->dev || g->host_sources_written) memset(psi.sources, 0, 6 * n * sizeof(float));
+    g->host_mirror_written = false;
+    g->host_sources_written = false;
+    g->fields_from_host = false;
 }
 
 double *timefield3d_get_fields(timefield3d psi)
@@ -378,31 +374,31 @@ FDTD_PLOT(timefield3d_plot_permittivity_z_slice, 2, 2, 0)
 // ============================================================================
 // materials (host rasterisers)
 // ============================================================================
-void timefield3d_set_background(timefield3d psi, float ep, float mu) { LOCK; raster_background(psi, ep, mu); mark_materials(psi); }
-void timefield3d_set_top_half_plane(timefield3d psi, float ep, float mu, int bottom) { LOCK; raster_top_half_plane(psi, ep, mu, bottom); mark_materials(psi); }
-void timefield3d_set_background_permittivity(timefield3d psi, float ep) { LOCK; raster_background_permittivity(psi, ep); mark_materials(psi); }
-void timefield3d_set_background_permeability(timefield3d psi, float mu) { LOCK; raster_background_permeability(psi, mu); mark_materials(psi); }
-void timefield3d_set_background_electric_conductivity(timefield3d psi, float sig) { LOCK; raster_background_conductivity(psi, sig, 0); mark_materials(psi); }
-void timefield3d_set_background_magnetic_conductivity(timefield3d psi, float sig) { LOCK; raster_background_conductivity(psi, sig, 1); mark_materials(psi); }
+void timefield3d_set_background(timefield3d psi, float ep, float mu) { LOCK; raster_background(psi, ep, mu); mark_materials(psi, kMatEp | kMatMu); }
+void timefield3d_set_top_half_plane(timefield3d psi, float ep, float mu, int bottom) { LOCK; raster_top_half_plane(psi, ep, mu, bottom); mark_materials(psi, kMatEp | kMatMu); }
+void timefield3d_set_background_permittivity(timefield3d psi, float ep) { LOCK; raster_background_permittivity(psi, ep); mark_materials(psi, kMatEp); }
+void timefield3d_set_background_permeability(timefield3d psi, float mu) { LOCK; raster_background_permeability(psi, mu); mark_materials(psi, kMatMu); }
+void timefield3d_set_background_electric_conductivity(timefield3d psi, float sig) { LOCK; raster_background_conductivity(psi, sig, 0); mark_materials(psi, kMatSig); }
+void timefield3d_set_background_magnetic_conductivity(timefield3d psi, float sig) { LOCK; raster_background_conductivity(psi, sig, 1); mark_materials(psi, kMatSig); }
 void timefield3d_set_background_complex_permittivity(timefield3d psi, double omega, float real_ep, float imag_ep)
 {
     // timefield3d.c:1448-1455
     LOCK;
     raster_background_permittivity(psi, real_ep);
     raster_background_conductivity(psi, (float)(omega * imag_ep), 0);
-    mark_materials(psi);
+    mark_materials(psi, kMatEp | kMatSig);
 }
 void timefield3d_set_prism_permittivity(timefield3d psi, float ep, int sx, int ex, int sy, int ey, int sz, int ez)
 {
     LOCK;
     raster_prism(psi, ep, sx, ex, sy, ey, sz, ez, 0);
-    mark_materials(psi);
+    mark_materials(psi, kMatEp);
 }
 void timefield3d_set_prism_electric_conductivity(timefield3d psi, float sig, int sx, int ex, int sy, int ey, int sz, int ez)
 {
     LOCK;
     raster_prism(psi, sig, sx, ex, sy, ey, sz, ez, 1);
-    mark_materials(psi);
+    mark_materials(psi, kMatSig);
 }
 void timefield3d_set_prism_complex_permittivity(timefield3d psi, double omega, float real_ep, float imag_ep, int sx,
                                                 int ex, int sy, int ey, int sz, int ez)
@@ -411,21 +407,21 @@ void timefield3d_set_prism_complex_permittivity(timefield3d psi, double omega, f
     LOCK;
     raster_prism(psi, real_ep, sx, ex, sy, ey, sz, ez, 0);
     raster_prism(psi, (float)(omega * imag_ep), sx, ex, sy, ey, sz, ez, 1);
-    mark_materials(psi);
+    mark_materials(psi, kMatEp | kMatSig);
 }
 void timefield3d_set_waveguide(timefield3d psi, float ep, int start_x, int end_x, int start_z, int end_z, int bottom, int top)
 {
     // timefield3d.c:1506-1509
     LOCK;
     raster_prism(psi, ep, start_x, end_x, bottom, top, start_z, end_z, 0);
-    mark_materials(psi);
+    mark_materials(psi, kMatEp);
 }
 void timefield3d_set_taper(timefield3d psi, double ep, double mu, int start_left, int start_right, int end_left,
                            int end_right, int start_z, int end_z, int bottom, int top)
 {
     LOCK;
     raster_taper(psi, ep, mu, start_left, start_right, end_left, end_right, start_z, end_z, bottom, top);
-    mark_materials(psi);
+    mark_materials(psi, kMatEp | kMatMu);
 }
 
 // ============================================================================
@@ -676,7 +672,7 @@ void adjoint3d_taper_insert(timefield3d psi, adjoint3d_taper taper)
 {
     LOCK;
     taper_insert(psi, taper);
-    mark_materials(psi);
+    mark_materials(psi, kMatEp | kMatMu);
 }
 
 static void taper_store(adjoint3d_taper taper, timefield3d psi, int timestep, int which)
@@ -838,7 +834,7 @@ int timefield3d_sync_device(timefield3d psi)
     LOCK;
     Grid *g = grid_lookup(psi);
     if (!g) return FDTD_ERR_ARG;
-    g->mat_dirty = true;
+    g->mat_dirty = kMatAll;
     g->fields_from_host = true;
     if (!grid_ensure_device(g)) return fdtd_last_error();
     // sources: every z-plane holding a non-zero host source value
@@ -883,6 +879,7 @@ int timefield3d_set_source_value(timefield3d psi, int i, int j, int k, int m, fl
     const long long nxy = (long long)psi.i * psi.j;
     launch_set_value(pl->p, m * nxy + i + (long long)psi.i * j, value, g->st);
     psi.sources[6 * (i + (long long)psi.i * (j + (long long)psi.j * k)) + m] = value;
+    g->host_sources_written = true;
     return cuda_ok(cudaGetLastError(), "set source") ? FDTD_OK : fdtd_last_error();
 }
 
@@ -1160,6 +1157,55 @@ int timefield3d_run(timefield3d psi, double delta_t, int nsteps)
         return FDTD_ERR_ARG;
     }
     return run_steps(g, delta_t, nsteps) ? FDTD_OK : fdtd_last_error();
+}
+
+int fdtd_set_device(int device)
+{
+    LOCK;
+    if (!device_available()) return fdtd_last_error();
+    return cuda_ok(cudaSetDevice(device), "cudaSetDevice") ? FDTD_OK : fdtd_last_error();
+}
+
+long long fdtd_launch_count(void) { return launch_count(); }
+
+void *timefield3d_get_stream(timefield3d psi)
+{
+    LOCK;
+    Grid *g = dev_grid(psi);
+    return g ? (void *)g->st : nullptr;
+}
+
+int timefield3d_upload_materials(timefield3d psi)
+{
+    LOCK;
+    Grid *g = dev_grid(psi);
+    if (!g) return fdtd_last_error();
+    return grid_upload_materials(g) ? FDTD_OK : fdtd_last_error();
+}
+
+int timefield3d_set_kernel_timing(timefield3d psi, int on)
+{
+    LOCK;
+    Grid *g = grid_lookup(psi);
+    if (!g) return FDTD_ERR_ARG;
+    if (g->dev && (!drain_kernel_timing(g, 0) || !drain_kernel_timing(g, 1))) return fdtd_last_error();
+    g->ktime = on != 0;
+    g->ktime_ms = 0;
+    g->ktime_n = 0;
+    return FDTD_OK;
+}
+
+int timefield3d_read_kernel_timing(timefield3d psi, double *total_ms, long long *count)
+{
+    LOCK;
+    Grid *g = grid_lookup(psi);
+    if (!g || !total_ms || !count) return FDTD_ERR_ARG;
+    if (g->dev && (!drain_kernel_timing(g, 0) || !drain_kernel_timing(g, 1))) return fdtd_last_error();
+    *total_ms = g->ktime_ms;
+    *count = g->ktime_n;
+    g->ktime_ms = 0;
+    g->ktime_n = 0;
+    return FDTD_OK;
 }
 
 int timefield3d_release_mode(mode m)

@@ -2,6 +2,7 @@
 // CUDA-graph capture of multi-step runs.
 #include "engine.h"
 
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -36,6 +37,10 @@ extern "C" void fdtd_clear_error(void)
 }
 
 namespace fdtd {
+
+static std::atomic<long long> g_launches{0};
+void note_launch(int n) { g_launches += n; }
+long long launch_count() { return g_launches.load(); }
 
 bool cuda_ok(cudaError_t e, const char *what)
 {
@@ -326,7 +331,11 @@ Grid::~Grid()
 {
     if (dev) {
         cudaStreamSynchronize(st);
-        if (graph) cudaGraphExecDestroy(graph);
+        for (int s = 0; s < 3; s++)
+            if (graph[s]) cudaGraphExecDestroy(graph[s]);
+        for (int s = 0; s < 2; s++)
+            for (int e = 0; e < 64; e++)
+                if (kev[s][e]) cudaEventDestroy(kev[s][e]);
         free_fields(this);
         for (int c = 0; c < 3; c++) { dfree(ep[c]); dfree(mu[c]); dfree(cb[c]); dfree(ca[c]); }
         for (int m = 0; m < 6; m++) dfree(sig[m]);
@@ -407,6 +416,7 @@ static bool upload_deinterleave(Grid *g, const float *host, int stride, float **
     float *d[6] = {};
     for (int c = 0; c < stride; c++) d[c] = dst[c];
     int blocks = (int)std::min<long long>((g->n + 255) / 256, 4736);
+    note_launch();
     k_deinterleave<<<blocks, 256, 0, g->st>>>((const float *)g->d_aos, stride, d[0], d[1], d[2], d[3], d[4], d[5],
                                                 g->n, ref, d_flags);
     CKL("k_deinterleave");
@@ -415,11 +425,21 @@ static bool upload_deinterleave(Grid *g, const float *host, int stride, float **
 
 bool grid_upload_materials(Grid *g)
 {
+    // only the arrays the rasterisers touched (kMatEp / kMatMu / kMatSig bits);
     // flags: [0..2] ep != 1, [3..5] mu != 1, [6..11] sig != 0 (bit 2: not finite)
-    CK(cudaMemsetAsync(g->d_flag, 0, 12 * sizeof(int), g->st));
-    if (!upload_deinterleave(g, g->h.ep, 3, g->ep, 1.0f, g->d_flag + 0)) return false;
-    if (!upload_deinterleave(g, g->h.mu, 3, g->mu, 1.0f, g->d_flag + 3)) return false;
-    if (!upload_deinterleave(g, g->h.sig, 6, g->sig, 0.0f, g->d_flag + 6)) return false;
+    const int dirty = g->mat_dirty;
+    if (dirty & kMatEp) {
+        CK(cudaMemsetAsync(g->d_flag + 0, 0, 3 * sizeof(int), g->st));
+        if (!upload_deinterleave(g, g->h.ep, 3, g->ep, 1.0f, g->d_flag + 0)) return false;
+    }
+    if (dirty & kMatMu) {
+        CK(cudaMemsetAsync(g->d_flag + 3, 0, 3 * sizeof(int), g->st));
+        if (!upload_deinterleave(g, g->h.mu, 3, g->mu, 1.0f, g->d_flag + 3)) return false;
+    }
+    if (dirty & kMatSig) {
+        CK(cudaMemsetAsync(g->d_flag + 6, 0, 6 * sizeof(int), g->st));
+        if (!upload_deinterleave(g, g->h.sig, 6, g->sig, 0.0f, g->d_flag + 6)) return false;
+    }
     CK(cudaMemcpyAsync(g->h_flag, g->d_flag, 12 * sizeof(int), cudaMemcpyDeviceToHost, g->st));
     CK(cudaStreamSynchronize(g->st));
     int any = 0;
@@ -431,7 +451,7 @@ bool grid_upload_materials(Grid *g)
     g->mu_nonunit = ((g->h_flag[3] | g->h_flag[4] | g->h_flag[5]) & 1) != 0;
     g->sig_e = ((g->h_flag[6] | g->h_flag[7] | g->h_flag[8]) & 1) != 0;
     g->sig_m = ((g->h_flag[9] | g->h_flag[10] | g->h_flag[11]) & 1) != 0;
-    g->mat_dirty = false;
+    g->mat_dirty = 0;
     g->coef_valid = false;
     g->version++;
     return true;
@@ -454,6 +474,7 @@ bool grid_download_fields(Grid *g)
     if (g->prec == FDTD_F64) launch_soa_to_aos<double>(g->d_aos, (double *const *)g->f[g->cur], g->n, g->st);
     else launch_soa_to_aos<float>(g->d_aos, (float *const *)g->f[g->cur], g->n, g->st);
     CKL("soa_to_aos");
+    g->host_mirror_written = true;
     CK(cudaMemcpyAsync(g->h.fields, g->d_aos, (size_t)g->n * 6 * sizeof(double), cudaMemcpyDeviceToHost, g->st));
     CK(cudaStreamSynchronize(g->st));
     return true;
@@ -501,7 +522,7 @@ bool grid_ensure_device(Grid *g)
         cudaHostRegister(g->h.mu, (size_t)g->n * 3 * sizeof(float), cudaHostRegisterDefault);
         cudaHostRegister(g->h.sig, (size_t)g->n * 6 * sizeof(float), cudaHostRegisterDefault);
         cudaGetLastError();
-        g->mat_dirty = true;
+        g->mat_dirty = kMatAll;
     }
     if (!g->f[0][0]) {
         if (!alloc_field_set(g, 0)) return false;
@@ -641,6 +662,7 @@ bool grid_prepare_step(Grid *g, double dt)
                 if (!dalloc(&g->cb[c], fb, g->st, false)) return false;
                 if (g->sig_e && !dalloc(&g->ca[c], fb, g->st, false)) return false;
                 int blocks = (int)std::min<long long>((g->n + 255) / 256, 4736);
+                note_launch();
                 k_coef<<<blocks, 256, 0, g->st>>>(g->ep[c], g->sig_e ? g->sig[c] : nullptr, g->cb[c],
                                                     g->sig_e ? g->ca[c] : nullptr, g->n, dt, g->dx);
                 CKL("k_coef");
@@ -828,10 +850,12 @@ bool enqueue_step(Grid *g, double dt, bool with_extras)
                            g->sched.reverse, g->sched.adjoint, g->st);
     }
     bool ok;
+    if (g->cap_ev) CK(cudaEventRecord(g->cap_ev[2 * g->cap_step], g->st));
     if (g->prec == FDTD_F64) ok = step_split<double>(g, dt);
     else if (fused_path(g)) ok = step_fused(g, dt);
     else ok = step_split<float>(g, dt);
     if (!ok) return false;
+    if (g->cap_ev) CK(cudaEventRecord(g->cap_ev[2 * g->cap_step + 1], g->st));
     return with_extras ? enqueue_after_step(g, dt) : true;
 }
 
@@ -856,43 +880,97 @@ static bool prepare_run(Grid *g, double dt)
     return true;
 }
 
+static constexpr int kGraphSteps = 32;   // steps per captured graph (even: the fused path ping-pongs)
+
+// capture kGraphSteps steps into g->graph[slot]; slots 1 and 2 also record an
+// event pair around each step's Yee update (kernel timing)
+static bool capture_graph(Grid *g, int slot, double dt)
+{
+    if (g->graph[slot] && g->graph_steps[slot] == kGraphSteps && g->graph_dt[slot] == dt &&
+        g->graph_version[slot] == g->version && g->graph_cur[slot] == g->cur)
+        return true;
+    if (g->graph[slot]) {
+        CK(cudaStreamSynchronize(g->st));
+        cudaGraphExecDestroy(g->graph[slot]);
+        g->graph[slot] = nullptr;
+    }
+    if (slot > 0) {
+        for (int e = 0; e < 2 * kGraphSteps; e++)
+            if (!g->kev[slot - 1][e]) CK(cudaEventCreate(&g->kev[slot - 1][e]));
+        g->kpending[slot - 1] = false;
+        g->cap_ev = g->kev[slot - 1];
+    }
+    const int cur0 = g->cur;
+    const long long before = launch_count();
+    cudaGraph_t gr;
+    CK(cudaStreamBeginCapture(g->st, cudaStreamCaptureModeThreadLocal));
+    bool ok = true;
+    for (int s = 0; s < kGraphSteps && ok; s++) {
+        g->cap_step = s;
+        ok = enqueue_step(g, dt, true);
+    }
+    g->cap_ev = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(g->st, &gr);
+    const long long nodes = launch_count() - before;
+    note_launch((int)-nodes);   // captured, not executed
+    if (!ok) {
+        if (ce == cudaSuccess) cudaGraphDestroy(gr);
+        g->cur = cur0;
+        return false;
+    }
+    CK(ce);
+    cudaError_t ie = cudaGraphInstantiate(&g->graph[slot], gr, 0);
+    cudaGraphDestroy(gr);
+    CK(ie);
+    g->graph_steps[slot] = kGraphSteps;
+    g->graph_dt[slot] = dt;
+    g->graph_version[slot] = g->version;
+    g->graph_cur[slot] = cur0;
+    g->graph_nodes[slot] = nodes;
+    if (g->cur != cur0) {
+        set_error(FDTD_ERR_CUDA, "internal: odd graph length");
+        return false;
+    }
+    return true;
+}
+
+// read the Yee-update times of timed graph `set` once it has completed
+bool drain_kernel_timing(Grid *g, int set)
+{
+    if (!g->kpending[set]) return true;
+    CK(cudaEventSynchronize(g->kev[set][2 * kGraphSteps - 1]));
+    for (int s = 0; s < kGraphSteps; s++) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, g->kev[set][2 * s], g->kev[set][2 * s + 1]));
+        g->ktime_ms += ms;
+        g->ktime_n++;
+    }
+    g->kpending[set] = false;
+    return true;
+}
+
 bool run_steps(Grid *g, double dt, int nsteps)
 {
     if (nsteps <= 0) return true;
     if (!prepare_run(g, dt)) return false;
-    const int G = 32;   // steps per captured graph (even: the fused path ping-pongs)
-    int full = nsteps / G, rest = nsteps % G;
-    if (full > 0) {
-        if (!g->graph || g->graph_steps != G || g->graph_dt != dt || g->graph_version != g->version ||
-            g->cur != 0) {
-            if (g->graph) {
-                cudaGraphExecDestroy(g->graph);
-                g->graph = nullptr;
-            }
-            int cur0 = g->cur;
-            cudaGraph_t gr;
-            CK(cudaStreamBeginCapture(g->st, cudaStreamCaptureModeThreadLocal));
-            bool ok = true;
-            for (int s = 0; s < G && ok; s++) ok = enqueue_step(g, dt, true);
-            cudaError_t ce = cudaStreamEndCapture(g->st, &gr);
-            if (!ok) {
-                if (ce == cudaSuccess) cudaGraphDestroy(gr);
-                g->cur = cur0;
-                return false;
-            }
-            CK(ce);
-            CK(cudaGraphInstantiate(&g->graph, gr, 0));
-            cudaGraphDestroy(gr);
-            g->graph_steps = G;
-            g->graph_dt = dt;
-            g->graph_version = g->version;
-            g->graph_cur = cur0;
-            if (g->cur != cur0) {
-                set_error(FDTD_ERR_CUDA, "internal: odd graph length");
-                return false;
-            }
+    int full = nsteps / kGraphSteps, rest = nsteps % kGraphSteps;
+    if (full > 0 && !g->ktime) {
+        if (!capture_graph(g, 0, dt)) return false;
+        for (int r = 0; r < full; r++) {
+            CK(cudaGraphLaunch(g->graph[0], g->st));
+            note_launch((int)g->graph_nodes[0]);
         }
-        for (int r = 0; r < full; r++) CK(cudaGraphLaunch(g->graph, g->st));
+    } else if (full > 0) {
+        // two graphs alternate: while one runs, the host reads the other's
+        // event times, so the device never waits for the host
+        if (!capture_graph(g, 1, dt) || !capture_graph(g, 2, dt)) return false;
+        for (int r = 0; r < full; r++) {
+            int set = r & 1;
+            if (!drain_kernel_timing(g, set)) return false;
+            CK(cudaGraphLaunch(g->graph[1 + set], g->st));
+            note_launch((int)g->graph_nodes[1 + set]);
+            g->kpending[set] = true;
+        }
     }
     for (int s = 0; s < rest; s++)
         if (!enqueue_step(g, dt, true)) return false;

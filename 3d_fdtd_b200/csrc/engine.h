@@ -43,6 +43,8 @@ const void *priv_mode_new(const mode &m);
 void priv_mode_free(const void *key);
 
 // ---- grid ------------------------------------------------------------------
+enum { kMatEp = 1, kMatMu = 2, kMatSig = 4, kMatAll = 7 };
+
 struct Plane {
     int k;
     float *p;
@@ -88,8 +90,10 @@ struct Grid {
     void *old[6] = {};        // Mur snapshot
     float *ep[3] = {}, *mu[3] = {}, *sig[6] = {};
     bool sig_e = false, sig_m = false, mu_nonunit = false;
-    bool mat_dirty = true;
+    int mat_dirty = kMatAll;          // host material arrays newer than the device copies
     bool fields_from_host = false;   // host mirror must be uploaded before next use
+    bool host_mirror_written = false; // a sync wrote psi.fields / fourier_fields
+    bool host_sources_written = false; // timefield3d_set_source_value wrote psi.sources
     void **d_fptr[2] = {};           // device arrays of the 6 field pointers per set
 
     // CPML
@@ -139,13 +143,23 @@ struct Grid {
     int *d_flag = nullptr;              // 12 material flags
     int *h_flag = nullptr;              // pinned
 
-    // captured step graphs
-    cudaGraphExec_t graph = nullptr;
-    int graph_steps = 0;
-    double graph_dt = 0;
-    uint64_t graph_version = 0;
-    int graph_cur = 0;
+    // captured step graphs: [0] untimed; [1],[2] alternate when kernel timing is on
+    cudaGraphExec_t graph[3] = {};
+    int graph_steps[3] = {};
+    double graph_dt[3] = {};
+    uint64_t graph_version[3] = {};
+    int graph_cur[3] = {};
+    long long graph_nodes[3] = {};      // kernel launches per replay
     uint64_t version = 1;               // bumped on any configuration change
+
+    // kernel timing: an event pair around the Yee update of every captured step
+    bool ktime = false;
+    cudaEvent_t kev[2][64] = {};        // per timed graph, 2 per step
+    bool kpending[2] = {false, false};
+    cudaEvent_t *cap_ev = nullptr;      // events of the graph being captured
+    int cap_step = 0;
+    double ktime_ms = 0;
+    long long ktime_n = 0;
 
     ~Grid();
 };
@@ -168,6 +182,7 @@ void grid_zero(Grid *g);
 bool enqueue_step(Grid *g, double dt, bool with_extras);
 bool enqueue_after_step(Grid *g, double dt);
 bool run_steps(Grid *g, double dt, int nsteps);
+bool drain_kernel_timing(Grid *g, int set);
 bool rebuild_jobs(Grid *g);
 
 // typed helpers

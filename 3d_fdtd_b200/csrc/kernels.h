@@ -6,6 +6,10 @@
 
 namespace fdtd {
 
+// host-side count of kernel launches issued by this library (engine.cu)
+void note_launch(int n = 1);
+long long launch_count();
+
 // one overlap reduction: plane cz of the grid against a device mode
 struct OverlapJob {
     int cx, cy, cz;

@@ -377,6 +377,7 @@ void launch_update_E(const GridView<T> &g, const CpmlView<T> &c, const SourcePla
 {
     dim3 grd = grid_for(g.nx, g.ny, k_lo, k_hi, g.nz), blk(kBX, kBY);
     if (grd.z == 0) return;
+    note_launch();
     if (expl) k_update_E<T, true, false, true><<<grd, blk, 0, st>>>(g, c, s, dt, divisor, k_lo, k_hi);
     else if (cpml) {
         if (sig) k_update_E<T, true, true, false><<<grd, blk, 0, st>>>(g, c, s, dt, divisor, k_lo, k_hi);
@@ -393,6 +394,7 @@ void launch_update_H(const GridView<T> &g, const CpmlView<T> &c, const SourcePla
 {
     dim3 grd = grid_for(g.nx, g.ny, k_lo, k_hi, g.nz), blk(kBX, kBY);
     if (grd.z == 0) return;
+    note_launch();
     if (expl) { k_update_H<T, true, true, false, true><<<grd, blk, 0, st>>>(g, c, s, dt, divisor, k_lo, k_hi); return; }
 #define FDTD_H(SG, MU_, CP) k_update_H<T, SG, MU_, CP, false><<<grd, blk, 0, st>>>(g, c, s, dt, divisor, k_lo, k_hi)
     if (sig) {
@@ -408,6 +410,7 @@ void launch_update_H(const GridView<T> &g, const CpmlView<T> &c, const SourcePla
 template <typename T>
 void launch_save_shell(const GridView<T> &g, cudaStream_t st)
 {
+    note_launch();
     k_save_shell<T><<<g.nz, 256, 0, st>>>(g);
 }
 
@@ -417,13 +420,17 @@ void launch_mur(const GridView<T> &g, T dt, T dx, int efield, int ks, int ke, cu
     const int lo = ks == 0, hi = ke == g.nz;
     const int mid0 = lo ? 2 : ks, mid1 = hi ? g.nz - 2 : ke;
     int nblk = lo + (mid1 > mid0 ? mid1 - mid0 : 0) + hi;
-    if (nblk > 0) k_mur<T><<<nblk, 256, 0, st>>>(g, dt, dx, efield, ks, ke);
+    if (nblk > 0) {
+        note_launch();
+        k_mur<T><<<nblk, 256, 0, st>>>(g, dt, dx, efield, ks, ke);
+    }
 }
 
 template <typename T>
 void launch_aos_to_soa(const double *aos, T *const d[6], long long n, cudaStream_t st)
 {
     int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+    note_launch();
     k_aos_to_soa<T><<<blocks, 256, 0, st>>>(aos, d[0], d[1], d[2], d[3], d[4], d[5], n);
 }
 
@@ -431,6 +438,7 @@ template <typename T>
 void launch_soa_to_aos(double *aos, T *const s[6], long long n, cudaStream_t st)
 {
     int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+    note_launch();
     k_soa_to_aos<T><<<blocks, 256, 0, st>>>(aos, s[0], s[1], s[2], s[3], s[4], s[5], n);
 }
 

@@ -1,0 +1,414 @@
+"""Benchmark of the FDTD hot path: the 200x160x400 Si taper (FP32, 12-cell CPML,
+mode source, 11-wavelength mode-overlap monitors), one bench step = one full
+6000-time-step forward simulation, through libfdtd_b200.so's C ABI.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    torchrun --nproc-per-node N bench.py --gpus N ...   (N > 1: one replica per GPU)
+
+Prints one JSON line (rank 0).  Metric: Yee Mcell-updates/s = nx*ny*nz*time_steps
+per second, whole job (all ranks).  Device timing: CUDA events on the engine's
+own stream, barrier + synchronize on both sides, max over ranks.  `e2e` repeats
+the step through the public API with the geometry re-rasterised on the host and
+uploaded (pinned host mirrors), the mode profiles uploaded and the monitor
+results read back, timed on the host clock.  `roofline` uses the Yee-update
+time measured live with event pairs inside the captured graphs of the timed
+runs.  `--impl reference` times the reference's own C/OpenMP step (built from
+its sources into oracle/_ref) on the host cores on the same grid.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import gzip
+import importlib
+import json
+import math
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+MODES = os.path.join(ROOT, "tests", "golden", "modes")
+REF_PI = 3.141592652
+
+# ---------------------------------------------------------------------------
+# the workload: Si strip taper 0.5 -> 3.0 um, 220 nm core, SiO2 cladding
+# ---------------------------------------------------------------------------
+W = dict(nx=200, ny=160, nz=400, dx=0.025, ep_clad=2.085, ep_core=12.1, core_y=(76, 85), cx=100, cy=80,
+         w_in=(90, 110), w_out=(40, 160), taper_z=(30, 370), cpml=12, src_z=20, launch_z=25, out_z=380,
+         lam0=1.55, bw=0.3, lams=[round(1.50 + 0.01 * l, 2) for l in range(11)], time_steps=6000)
+WORKLOAD_NAME = "si_taper_200x160x400_dx25nm_cpml12_fp32_11lambda"
+
+
+def cell_axes_in_pml(nx, ny, nz, L):
+    return 2 * L * ny * nz + nx * 2 * L * nz + nx * ny * 2 * L
+
+
+def algorithmic_bytes_per_step(nx, ny, nz, L):
+    """60 B per cell (6 field components read + written, 3 E coefficients) and
+    32 B per (cell, CPML axis) (4 auxiliaries read + written), FP32."""
+    return 60 * nx * ny * nz + 32 * cell_axes_in_pml(nx, ny, nz, L)
+
+
+def source_tables(T, dt):
+    w0 = 2 * REF_PI / W["lam0"]
+    dw = 2 * math.pi * W["bw"] / W["lam0"] ** 2
+    sigma_n = (2 * math.sqrt(2 * math.log(2)) / dw) / dt
+    n0 = 3 * sigma_n
+    n = np.arange(T, dtype=np.float64)
+    amp = np.exp(-((n - n0) ** 2) / (2 * sigma_n ** 2))
+    phase = n * dt * w0
+    return amp, phase
+
+
+def rasterise(lib, t):
+    """Geometry through the reference's rasterisers (timefield3d.c:1356-1535)."""
+    b, top = W["core_y"]
+    z0, z1 = W["taper_z"]
+    lib.timefield3d_set_background(t, W["ep_clad"], 1.0)
+    lib.timefield3d_set_waveguide(t, W["ep_core"], W["w_in"][0], W["w_in"][1], 0, z0, b, top)
+    lib.timefield3d_set_taper(t, W["ep_core"], 1.0, W["w_in"][0], W["w_in"][1], W["w_out"][0], W["w_out"][1],
+                              z0, z1, b, top)
+    lib.timefield3d_set_waveguide(t, W["ep_core"], W["w_out"][0], W["w_out"][1], z1, W["nz"], b, top)
+
+
+def dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+        if shutil.which("nvidia-smi") is None:
+            return
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if gpu_id:
+            cmd += ["-i", gpu_id]
+        self.fh = open(self.path, "w")
+        self.proc = subprocess.Popen(cmd, stdout=self.fh, stderr=subprocess.DEVNULL)
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, v in zip(self.NAMES, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# the reference's own C (CPU baseline and --impl reference)
+# ---------------------------------------------------------------------------
+def reference_throughput(max_seconds: float, min_steps: int, max_steps: int, threads: int) -> dict:
+    """The reference's step + mode source + two mode overlaps per time step on the
+    same grid (Mur boundary: the reference has no CPML), on `threads` cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from bindings import Complex, Reference
+    R = Reference()
+    R.set_threads(threads)
+    nx, ny, nz, dx = W["nx"], W["ny"], W["nz"], W["dx"]
+    dt = 0.99 * dx / math.sqrt(3)
+    tf = R.timefield3d_new(nx, ny, nz, dx)
+    rasterise(R.lib, tf)
+    tmp = tempfile.mkdtemp()
+    modes = []
+    for name in ("c1_in_te0", "c1_out_te0"):
+        txt = os.path.join(tmp, name + ".txt")
+        with gzip.open(os.path.join(MODES, name + ".txt.gz"), "rb") as fi, open(txt, "wb") as fo:
+            shutil.copyfileobj(fi, fo)
+        modes.append(R.load_mode(txt))
+    shutil.rmtree(tmp)
+    amp, phase = source_tables(max_steps + 1, dt)
+    acc = [Complex(), Complex()]
+    n = 0
+    t0 = time.perf_counter()
+    while n < max_steps and (n < min_steps or time.perf_counter() - t0 < max_seconds):
+        R.timefield3d_mode_source(tf, W["cx"], W["cy"], W["src_z"], modes[0], phase[n], amp[n], 0)
+        R.timefield3d_apply_timestep_omp_full(tf, dt)
+        R.timefield3d_mode_overlap(tf, W["cx"], W["cy"], W["launch_z"], modes[0], phase[n], 0, C.byref(acc[0]))
+        R.timefield3d_mode_overlap(tf, W["cx"], W["cy"], W["out_z"], modes[1], phase[n], 0, C.byref(acc[1]))
+        n += 1
+    el = time.perf_counter() - t0
+    R.timefield3d_free(tf)
+    return {"mcells": nx * ny * nz * n / el / 1e6, "steps": n, "seconds": el, "threads": threads}
+
+
+def reference_arm(args, rank: int) -> None:
+    if rank != 0:
+        return
+    threads = max(1, min(os.cpu_count() or 1, W["nz"] // 2))
+    vals = []
+    for s in range(args.warmup + args.steps):
+        r = reference_throughput(1e9, 3, 3, threads)
+        if s >= args.warmup:
+            vals.append(r)
+    v = statistics.median([r["mcells"] for r in vals])
+    ms = statistics.median([r["seconds"] / r["steps"] * W["time_steps"] * 1e3 for r in vals])
+    sample = f"3 of {W['time_steps']} time steps per bench step (grid {W['nx']}x{W['ny']}x{W['nz']}, " \
+             "reference Mur boundary, mode source + 2 overlaps per time step), extrapolated"
+    line = {"impl": "reference", "metric": "Yee Mcell-updates/s", "value": v, "unit": "Mcell-updates/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_block(args),
+            "cpu_baseline": {"value": v, "unit": "Mcell-updates/s", "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_block(args) -> dict:
+    return {"workload": WORKLOAD_NAME, "grid": [W["nx"], W["ny"], W["nz"]], "dx_um": W["dx"],
+            "time_steps": args.time_steps, "cpml_cells": W["cpml"], "n_lambda": len(W["lams"]),
+            "lambda_um": [W["lams"][0], W["lams"][-1]], "fields": "f32", "monitors": "f64 compensated",
+            "taper_um": [0.5, 3.0], "taper_length_um": (W["taper_z"][1] - W["taper_z"][0]) * W["dx"],
+            "l2": "inputs larger than L2 (fields 307 MB, no flush needed)",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+# ---------------------------------------------------------------------------
+# our engine
+# ---------------------------------------------------------------------------
+class Taper:
+    """One simulation of the workload on one GPU."""
+
+    def __init__(self, fd, time_steps: int):
+        self.fd, self.T = fd, time_steps
+        lib = fd.lib
+        nx, ny, nz, dx = W["nx"], W["ny"], W["nz"], W["dx"]
+        self.dt = 0.99 * dx / math.sqrt(3)
+        self.grid = fd.Grid(nx, ny, nz, dx, fd.F32)
+        self.t = self.grid.t
+        rasterise(lib, self.t)
+        fd.call("timefield3d_set_cpml", self.t, W["cpml"], 3, -1.0, 1.0, 0.0)
+        self.mode_in = fd.read_mode_file(os.path.join(MODES, "c1_in_te0.txt.gz"))
+        self.mode_out = fd.read_mode_file(os.path.join(MODES, "c1_out_te0.txt.gz"))
+        self.amp, self.phase = source_tables(time_steps, self.dt)
+        self.omega = np.array([2 * REF_PI / l for l in W["lams"]])
+        fd.call("timefield3d_upload_materials", self.t)
+        self.set_inputs()
+
+    def set_inputs(self):
+        fd, t = self.fd, self.t
+        fd.call("timefield3d_clear_monitors", t)
+        self.mon_in = fd.call("timefield3d_add_overlap_monitor", t, W["cx"], W["cy"], W["launch_z"],
+                              self.mode_in.copy().struct, 0, len(self.omega), dptr(self.omega))
+        self.mon_out = fd.call("timefield3d_add_overlap_monitor", t, W["cx"], W["cy"], W["out_z"],
+                               self.mode_out.copy().struct, 0, len(self.omega), dptr(self.omega))
+        fd.call("timefield3d_set_source_schedule", t, W["cx"], W["cy"], W["src_z"], self.mode_in.copy().struct, 0, 0,
+                self.T, dptr(self.amp), dptr(self.phase))
+
+    def h2d_bytes(self):
+        n = W["nx"] * W["ny"] * W["nz"]
+        # ep + mu (the rasterisers touch both), the input mode twice (source schedule,
+        # launch monitor), the output mode once, the source table, the frequencies
+        modes = 2 * 6 * 16 * self.mode_in.mi * self.mode_in.mj + 6 * 16 * self.mode_out.mi * self.mode_out.mj
+        return 2 * 3 * 4 * n + modes + 3 * 8 * self.T + 2 * 8 * len(self.omega)
+
+    def d2h_bytes(self):
+        return 2 * 2 * 16 * len(self.omega)
+
+    def run(self):
+        self.fd.lib.timefield3d_zero_fields(self.t)
+        self.fd.call("timefield3d_run", self.t, self.dt, self.T)
+
+    def transmission(self):
+        a, b = (self.fd.Complex * len(self.omega))(), (self.fd.Complex * len(self.omega))()
+        self.fd.call("timefield3d_read_overlap_monitor", self.t, self.mon_in, a)
+        self.fd.call("timefield3d_read_overlap_monitor", self.t, self.mon_out, b)
+        oi = np.array([complex(x.re, x.im) for x in a])
+        oo = np.array([complex(x.re, x.im) for x in b])
+        return np.abs(oo / oi) ** 2
+
+    def e2e_step(self):
+        """Design evaluation through the public API: re-rasterise, upload, run, read."""
+        rasterise(self.fd.lib, self.t)
+        self.fd.call("timefield3d_upload_materials", self.t)
+        self.set_inputs()
+        self.run()
+        return self.transmission()
+
+
+def read_traffic(kernel_tag: str):
+    """DRAM bytes per Yee step from the committed ncu summary of this workload, or None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel_tag}.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_step:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        p = json.load(open(path))
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def our_arm(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+    fd = importlib.import_module("3d_fdtd_b200")
+    if fd.lib.fdtd_device_count() <= 0:
+        raise SystemExit("bench: no CUDA device")
+    torch.cuda.set_device(local_rank)
+    fd.call("fdtd_set_device", local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    sim = Taper(fd, args.time_steps)
+    stream = torch.cuda.ExternalStream(fd.lib.timefield3d_get_stream(sim.t))
+    cells = W["nx"] * W["ny"] * W["nz"]
+    # warm-up: full runs (graph capture, clocks)
+    for _ in range(args.warmup):
+        sim.run()
+    barrier()
+    # timed: K full runs on the engine's stream
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    fd.call("timefield3d_set_kernel_timing", sim.t, 1)
+    l0 = fd.lib.fdtd_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        sim.run()
+    ev1.record(stream)
+    ev1.synchronize()
+    barrier()
+    launches = fd.lib.fdtd_launch_count() - l0
+    clk = clocks.stop()
+    ktot, kcnt = C.c_double(), C.c_longlong()
+    fd.call("timefield3d_read_kernel_timing", sim.t, C.byref(ktot), C.byref(kcnt))
+    fd.call("timefield3d_set_kernel_timing", sim.t, 0)
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = world * cells * args.time_steps * args.steps / (ms / 1e3) / 1e6
+    trans = sim.transmission()
+    # roofline of the Yee update (E + H kernels with CPML), measured inside the timed runs
+    kms = ktot.value / max(kcnt.value, 1)
+    bytes_step = algorithmic_bytes_per_step(W["nx"], W["ny"], W["nz"], W["cpml"])
+    achieved = bytes_step / (kms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    kernel_tag = "yee_step_si_taper_200x160x400_fp32"
+    traffic = read_traffic(kernel_tag)
+    # end to end through the public API, host clock
+    barrier()
+    sim.e2e_step()   # warm
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        trans_e2e = sim.e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = world * cells * args.time_steps * args.steps / e2e_s / 1e6
+    # CPU baseline: the reference on this host's cores (rank 0, N = 1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = max(1, min(os.cpu_count() or 1, W["nz"] // 2))
+        r = reference_throughput(args.cpu_seconds, 3, 200, threads)
+        cpu = {"value": r["mcells"], "unit": "Mcell-updates/s", "cores": threads, "kind": "reference",
+               "sample": f"{r['steps']} of {W['time_steps']} time steps of the same grid in {r['seconds']:.1f} s "
+                         "(reference step with its Mur boundary, mode source and 2 overlaps per time step)"}
+    if rank == 0:
+        line = {"metric": "Yee Mcell-updates/s", "value": value, "unit": "Mcell-updates/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded geometry and mode profiles generated by the reference's mode solver)",
+                "config": config_block(args),
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                             "kernel": "Yee step (E and H update kernels, CPML terms)",
+                             "bytes_per_launch": bytes_step, "avg_launch_ms": kms,
+                             "timed_launches": kcnt.value},
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e, "unit": "Mcell-updates/s", "h2d_bytes_per_step": sim.h2d_bytes(),
+                        "d2h_bytes_per_step": sim.d2h_bytes()},
+                "gpu_launches": launches, "clocks": clk,
+                "transmission": {"lambda_um": W["lams"], "T": [round(float(x), 6) for x in trans],
+                                 "T_e2e_equal": bool(np.allclose(trans, trans_e2e, rtol=1e-6))}}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--time-steps", type=int, default=W["time_steps"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.gpus != world and world > 1:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE {world}")
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+    our_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -283,6 +283,20 @@ int timefield3d_run(timefield3d psi, double delta_t, int nsteps);
 
 /* forget the device copy of a mode (call after editing mode.fields in place) */
 int timefield3d_release_mode(mode m);
+
+/* CUDA device used by grids created afterwards on this thread */
+int fdtd_set_device(int device);
+/* kernels this library has launched so far (graph replays counted per kernel) */
+long long fdtd_launch_count(void);
+/* the grid's CUDA stream (cudaStream_t), for callers that order work or time it */
+void *timefield3d_get_stream(timefield3d psi);
+/* upload psi.ep/mu/sig now (otherwise done on the next device use after a change) */
+int timefield3d_upload_materials(timefield3d psi);
+/* Kernel timing: while on, every captured step of timefield3d_run records a CUDA
+ * event pair around its Yee update (E and H kernels, boundary included); read
+ * returns the summed milliseconds and the number of timed steps, then resets. */
+int timefield3d_set_kernel_timing(timefield3d psi, int on);
+int timefield3d_read_kernel_timing(timefield3d psi, double *total_ms, long long *count);
 /* copy the device edge storage into taper.forward_fields/adjoint_fields in the
  * reference layout [t][k][j][edge][6] (E components; H left zero) */
 int adjoint3d_taper_sync_host(adjoint3d_taper taper);

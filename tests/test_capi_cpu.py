@@ -59,10 +59,8 @@ def test_taper_insert_and_slice_writer_match_reference(fd, ref):
     dims = (40, 20, 60, 0.02)
     left, right = [12, 10, 9, 11, 12], [28, 29, 31, 30, 28]
     out = []
-    for lib, newgrid in ((fd.lib, lambda: fd.Grid(*dims).t), (ref.lib, lambda: ref.timefield3d_new(*dims))):
-        keep = []
-        t = newgrid()
-        keep.append(t)
+    ours = fd.Grid(*dims)       # owns the host arrays for the whole test
+    for lib, t in ((fd.lib, ours.t), (ref.lib, ref.timefield3d_new(*dims))):
         lib.timefield3d_set_background(t, 2.085, 1.0)
         tp = lib.adjoint3d_taper_new(12.1, 1.0, 4, 10, 50, (C.c_int * 5)(*left), (C.c_int * 5)(*right), 8, 12, 5)
         lib.adjoint3d_taper_insert(t, tp)

@@ -850,12 +850,14 @@ bool enqueue_step(Grid *g, double dt, bool with_extras)
                            g->sched.reverse, g->sched.adjoint, g->st);
     }
     bool ok;
-    if (g->cap_ev) CK(cudaEventRecord(g->cap_ev[2 * g->cap_step], g->st));
+    // External: captured as an event-record node whose timestamp the host can
+    // read after a replay (a plain record during capture is only a dependency)
+    if (g->cap_ev) CK(cudaEventRecordWithFlags(g->cap_ev[2 * g->cap_step], g->st, cudaEventRecordExternal));
     if (g->prec == FDTD_F64) ok = step_split<double>(g, dt);
     else if (fused_path(g)) ok = step_fused(g, dt);
     else ok = step_split<float>(g, dt);
     if (!ok) return false;
-    if (g->cap_ev) CK(cudaEventRecord(g->cap_ev[2 * g->cap_step + 1], g->st));
+    if (g->cap_ev) CK(cudaEventRecordWithFlags(g->cap_ev[2 * g->cap_step + 1], g->st, cudaEventRecordExternal));
     return with_extras ? enqueue_after_step(g, dt) : true;
 }
 

@@ -224,6 +224,29 @@ def test_wg_adjoint_gradient_golden(fd, orc, gpu):
     fd.lib.adjoint3d_taper_free(taper)
 
 
+def test_kernel_timing_run_equals_untimed(fd, gpu):
+    """Timed graphs (event pairs around each Yee update) compute the same fields."""
+    outs = []
+    for timed in (False, True):
+        grid = fd.Grid(24, 20, 28, 0.02, fd.F32)
+        lossy_problem(fd.lib, grid.t)
+        fd.call("timefield3d_set_cpml", grid.t, 4, 3, -1.0, 1.0, 0.0)
+        fd.call("timefield3d_set_source_value", grid.t, 10, 9, 14, 2, 1.0)
+        fd.call("timefield3d_set_kernel_timing", grid.t, int(timed))
+        l0 = fd.lib.fdtd_launch_count()
+        fd.call("timefield3d_run", grid.t, DT_FACTOR * 0.02, 100)
+        ms, cnt = C.c_double(), C.c_longlong()
+        fd.call("timefield3d_read_kernel_timing", grid.t, C.byref(ms), C.byref(cnt))
+        launches = fd.lib.fdtd_launch_count() - l0
+        assert launches >= 100 * 2
+        if timed:
+            assert cnt.value == 96 and ms.value > 0
+        else:
+            assert cnt.value == 0
+        outs.append(grid.fields())
+    assert np.array_equal(outs[0], outs[1])
+
+
 def test_run_graph_equals_stepwise(fd, gpu):
     """timefield3d_run (scheduled source, graphs, monitors, bound store) equals the per-call path."""
     p = wg_setup()

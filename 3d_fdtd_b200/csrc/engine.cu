@@ -465,6 +465,7 @@ bool grid_upload_fields(Grid *g)
     else launch_aos_to_soa<float>(g->d_aos, (float *const *)g->f[g->cur], g->n, g->st);
     CKL("aos_to_soa");
     g->fields_from_host = false;
+    g->pp_synced = false;
     return true;
 }
 
@@ -655,7 +656,25 @@ bool grid_prepare_step(Grid *g, double dt)
         if (g->prof_dt != dt && !build_profiles(g, dt)) return false;
     }
     if (fused) {
-        if (!g->f[1][0] && !alloc_field_set(g, 1)) return false;
+        if (!g->f[1][0]) {
+            if (!alloc_field_set(g, 1)) return false;
+            g->pp_synced = false;
+        }
+        if (!g->pp_synced) {
+            // the fused kernel writes only interior cells: start both sets equal
+            const int a = g->cur, b = 1 - g->cur;
+            const size_t fb = (size_t)g->n * sizeof(float);
+            for (int m = 0; m < 6; m++) CK(cudaMemcpyAsync(g->f[b][m], g->f[a][m], fb, cudaMemcpyDeviceToDevice, g->st));
+            if (g->boundary == FDTD_BOUNDARY_CPML) {
+                size_t L2 = 2 * (size_t)g->L;
+                size_t sz[3] = {L2 * g->ny * g->nz, (size_t)g->nx * L2 * g->nz, (size_t)g->nx * g->ny * L2};
+                for (int ax = 0; ax < 3; ax++)
+                    for (int w = 0; w < 4; w++)
+                        CK(cudaMemcpyAsync(g->psi[b][ax][w], g->psi[a][ax][w], sz[ax] * sizeof(float),
+                                           cudaMemcpyDeviceToDevice, g->st));
+            }
+            g->pp_synced = true;
+        }
         if (!g->coef_valid || g->coef_dt != dt) {
             size_t fb = (size_t)g->n * sizeof(float);
             for (int c = 0; c < 3; c++) {

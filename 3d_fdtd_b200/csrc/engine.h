@@ -95,6 +95,7 @@ struct Grid {
     bool host_mirror_written = false; // a sync wrote psi.fields / fourier_fields
     bool host_sources_written = false; // timefield3d_set_source_value wrote psi.sources
     void **d_fptr[2] = {};           // device arrays of the 6 field pointers per set
+    bool pp_synced = false;          // set 1-cur equals set cur on the shell (fused path)
 
     // CPML
     int L = 0, order = 3;

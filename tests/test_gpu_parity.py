@@ -94,6 +94,53 @@ def test_cpml_f32_close(fd, orc, gpu):
     assert err < 2e-5, err
 
 
+def fused_problem(lib, t, dims, lossy):
+    nx, ny, nz = dims
+    lib.timefield3d_set_background(t, 1.0, 1.0)
+    lib.timefield3d_set_prism_permittivity(t, 4.0, nx // 4, 3 * nx // 4, ny // 4, 3 * ny // 4, nz // 4, nz // 2)
+    lib.timefield3d_set_top_half_plane(t, 2.25, 1.0, 2 * ny // 3)
+    if lossy:
+        lib.timefield3d_set_prism_electric_conductivity(t, 0.4, nx // 3, nx // 2, ny // 3, ny // 2, nz // 3, nz // 2)
+
+
+@pytest.mark.parametrize("dims,boundary,lossy", [((37, 19, 45), "cpml", False), ((64, 40, 150), "cpml", True),
+                                                  ((33, 17, 40), "pec", False)])
+def test_fused_f32_matches_oracle(fd, orc, gpu, dims, boundary, lossy):
+    """FP32 single-pass kernel (mu = 1, no magnetic loss) against the FP64 restatement."""
+    nx, ny, nz = dims
+    dx = 0.02
+    dt = DT_FACTOR * dx
+    grid = fd.Grid(nx, ny, nz, dx, fd.F32)
+    fused_problem(fd.lib, grid.t, dims, lossy)
+    g = oracle_copy(orc, grid)
+    if boundary == "cpml":
+        fd.call("timefield3d_set_cpml", grid.t, 6, 3, -1.0, 2.0, 0.1)
+        g.set_boundary(orc.CPML)
+        g.set_cpml(6, 3, -1.0, 2.0, 0.1, dt)
+    else:
+        fd.call("timefield3d_set_boundary", grid.t, fd.PEC)
+        g.set_boundary(orc.PEC)
+    src = [(nx // 2, ny // 2, nz // 3, 2, 1.0), (nx // 2 - 3, ny // 2 + 1, nz // 3, 4, 0.5),
+           (nx // 3, ny // 3, 2 * nz // 3, 0, -0.7)]
+    steps = 160
+    launches = []
+    for n in range(steps):
+        J = drive(n)
+        for (i, j, k, m, s) in src:
+            fd.lib.timefield3d_set_source_value(grid.t, i, j, k, m, s * J)
+            g.src[m][k, j, i] = np.float32(s * J)
+        l0 = fd.lib.fdtd_launch_count()
+        fd.lib.timefield3d_apply_timestep_omp_full(grid.t, dt)
+        launches.append(fd.lib.fdtd_launch_count() - l0)
+        g.step(dt)
+    fd.check("fused loop")
+    assert max(launches[5:]) == 2          # one Yee kernel + the step counter
+    a, b = grid.fields(), g.fields()
+    err = np.abs(a - b).max() / np.abs(b).max()
+    assert np.abs(b).max() > 1e-3
+    assert err < 5e-5, err
+
+
 def test_c0_probes_golden(fd, gpu):
     """64^3 dipole, 1000 FP64 steps: probe series equal the reference's."""
     gold = np.load(os.path.join(GOLDEN, "c0_probes.npz"))

@@ -825,7 +825,7 @@ int timefield3d_sync_host(timefield3d psi)
     Grid *g = grid_lookup(psi);
     if (!g) return FDTD_ERR_ARG;
     if (!g->dev || !g->f[g->cur][0]) return FDTD_OK;
-    if (!grid_download_fields(g) || !sync_fourier_host(g)) return fdtd_last_error();
+    if (!grid_check_device_error(g) || !grid_download_fields(g) || !sync_fourier_host(g)) return fdtd_last_error();
     return FDTD_OK;
 }
 
@@ -862,7 +862,8 @@ int timefield3d_synchronize(timefield3d psi)
     Grid *g = grid_lookup(psi);
     if (!g) return FDTD_ERR_ARG;
     if (!g->dev) return FDTD_OK;
-    return cuda_ok(cudaStreamSynchronize(g->st), "cudaStreamSynchronize") ? FDTD_OK : fdtd_last_error();
+    if (!cuda_ok(cudaStreamSynchronize(g->st), "cudaStreamSynchronize")) return fdtd_last_error();
+    return grid_check_device_error(g) ? FDTD_OK : fdtd_last_error();
 }
 
 int timefield3d_set_source_value(timefield3d psi, int i, int j, int k, int m, float value)
@@ -952,7 +953,7 @@ int timefield3d_read_probe(timefield3d psi, int id, double *out, int count)
         return FDTD_ERR_ARG;
     }
     int n = std::min(count, g->probe_cap);
-    if (!cuda_ok(cudaStreamSynchronize(g->st), "sync") ||
+    if (!grid_check_device_error(g) ||
         !cuda_ok(cudaMemcpy(out, g->d_probe_buf + (size_t)id * g->probe_cap, n * sizeof(double), cudaMemcpyDeviceToHost), "probe D2H"))
         return fdtd_last_error();
     return FDTD_OK;
@@ -1026,7 +1027,7 @@ int timefield3d_read_overlap_monitor(timefield3d psi, int id, complex *out)
     }
     Monitor &mn = g->monitors[id];
     std::vector<double2> acc(2 * mn.nfreq);
-    if (!cuda_ok(cudaStreamSynchronize(g->st), "sync") ||
+    if (!grid_check_device_error(g) ||
         !cuda_ok(cudaMemcpy(acc.data(), mn.d_acc, acc.size() * sizeof(double2), cudaMemcpyDeviceToHost), "monitor D2H"))
         return fdtd_last_error();
     for (int f = 0; f < mn.nfreq; f++) {

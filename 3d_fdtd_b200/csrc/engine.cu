@@ -344,6 +344,10 @@ Grid::~Grid()
         dfree(d_step); dfree(d_jobs); dfree(d_job1); dfree(d_partials); dfree(d_inst);
         if (h_inst) cudaFreeHost(h_inst);
         if (h_flag) cudaFreeHost(h_flag);
+        if (h_err) cudaFreeHost(h_err);
+        dfree(d_err);
+        delete fmaps[0];
+        delete fmaps[1];
         dfree(d_flag);
         for (auto &mn : monitors) { dfree(mn.d_omega); dfree(mn.d_acc); priv_mode_free(mn.mode_key); }
         dfree(d_probes); dfree(d_probe_buf); dfree(d_probe_count);
@@ -457,6 +461,20 @@ bool grid_upload_materials(Grid *g)
     return true;
 }
 
+// waits for the grid, then reports (and clears) a bounded device wait that gave up
+bool grid_check_device_error(Grid *g)
+{
+    if (!g->dev || !g->d_err) return true;
+    CK(cudaMemcpyAsync(g->h_err, g->d_err, sizeof(int), cudaMemcpyDeviceToHost, g->st));
+    CK(cudaStreamSynchronize(g->st));
+    if (*g->h_err) {
+        CK(cudaMemsetAsync(g->d_err, 0, sizeof(int), g->st));
+        set_error(FDTD_ERR_TIMEOUT, "a device-side wait gave up; results since the last check are invalid");
+        return false;
+    }
+    return true;
+}
+
 bool grid_upload_fields(Grid *g)
 {
     if (!dalloc(&g->d_aos, (size_t)g->n * 6 * sizeof(double), g->st, false)) return false;
@@ -512,6 +530,8 @@ bool grid_ensure_device(Grid *g)
         if (!dalloc(&g->d_flag, 12 * sizeof(int), g->st)) return false;
         CK(cudaMallocHost(&g->h_flag, 12 * sizeof(int)));
         CK(cudaMallocHost(&g->h_inst, sizeof(double2)));
+        CK(cudaMallocHost(&g->h_err, sizeof(int)));
+        if (!dalloc(&g->d_err, sizeof(int), g->st)) return false;
         if (!dalloc(&g->d_inst, sizeof(double2), g->st)) return false;
         if (!dalloc(&g->d_job1, sizeof(OverlapJob), g->st)) return false;
         g->jobs_cap = 8;
@@ -688,6 +708,28 @@ bool grid_prepare_step(Grid *g, double dt)
             }
             g->coef_valid = true;
             g->coef_dt = dt;
+            // TMA descriptors (host-side encode; they only depend on the buffers)
+            delete g->fmaps[0];
+            delete g->fmaps[1];
+            g->fmaps[0] = g->fmaps[1] = nullptr;
+            if (fused_tma_supported(g->nx, g->ny, g->nz)) {
+                for (int s = 0; s < 2; s++) {
+                    FusedMaps *m = new FusedMaps();
+                    const float *ca3[3] = {g->sig_e ? g->ca[0] : nullptr, g->sig_e ? g->ca[1] : nullptr,
+                                           g->sig_e ? g->ca[2] : nullptr};
+                    if (!fused_make_maps(m, (const float *const *)g->f[s], g->cb, ca3, g->nx, g->ny, g->nz)) {
+                        delete m;
+                        m = nullptr;
+                    }
+                    g->fmaps[s] = m;
+                }
+                if (!g->fmaps[0] || !g->fmaps[1]) {
+                    delete g->fmaps[0];
+                    delete g->fmaps[1];
+                    g->fmaps[0] = g->fmaps[1] = nullptr;
+                }
+            }
+            g->version++;
         }
     }
     // overlap scratch for the monitors
@@ -795,7 +837,8 @@ static bool step_fused(Grid *g, double dt)
         for (int w = 0; w < 6; w++) a.prof[w][ax] = (const float *)g->prof[w][ax];
     }
     a.src = source_table(g);
-    launch_fused_step(a, g->st);
+    if (g->fmaps[in]) launch_fused_step_tma(a, *g->fmaps[in], g->d_err, g->st);
+    else launch_fused_step(a, g->st);
     CKL("fused step");
     g->cur = out;
     return true;

@@ -108,6 +108,9 @@ struct Grid {
     float *cb[3] = {}, *ca[3] = {};
     double coef_dt = 0;
     bool coef_valid = false;
+    FusedMaps *fmaps[2] = {};        // TMA descriptors with set s as input (null: cp.async kernel)
+    int *d_err = nullptr;            // device error flag (a bounded wait gave up)
+    int *h_err = nullptr;            // pinned
 
     // sources
     std::vector<Plane> planes;
@@ -173,6 +176,7 @@ void grid_unregister(const timefield3d &psi);
 bool grid_ensure_device(Grid *g);              // allocate device arrays, upload what is dirty
 bool grid_upload_materials(Grid *g);
 bool grid_upload_fields(Grid *g);              // host mirror -> device
+bool grid_check_device_error(Grid *g);         // waits; FDTD_ERR_TIMEOUT if a device wait gave up
 bool grid_download_fields(Grid *g);            // device -> host mirror (waits)
 bool grid_set_precision(Grid *g, int prec);
 bool grid_prepare_step(Grid *g, double dt);    // profiles / coefficients for dt

@@ -1,6 +1,7 @@
 // kernels.h -- host-side launchers of the device kernels (internal header).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include "common.cuh"
 
@@ -57,6 +58,18 @@ struct FusedArgs {
 };
 int fused_supported(int nx, int ny, int nz);
 void launch_fused_step(const FusedArgs &a, cudaStream_t st);
+
+// yee_fused_tma.cu (the same step with TMA staging; needs nx % 4 == 0)
+struct FusedMaps {
+    CUtensorMap h[3];    // H components of the input set, box (TX+8) x (TY+2)
+    CUtensorMap e[3];    // E components of the input set, box (TX+4) x (TY+1)
+    CUtensorMap cb[3];
+    CUtensorMap ca[3];
+};
+int fused_tma_supported(int nx, int ny, int nz);
+bool fused_make_maps(FusedMaps *m, const float *const f[6], const float *const cb[3], const float *const ca[3],
+                     int nx, int ny, int nz);
+void launch_fused_step_tma(const FusedArgs &a, const FusedMaps &m, int *err, cudaStream_t st);
 
 // aux_kernels.cu
 void launch_mode_source(float *plane, const float *const ep_plane[3], const float *const mu_plane[3], int nx, int ny,

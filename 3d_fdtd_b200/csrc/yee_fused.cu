@@ -283,48 +283,52 @@ k_fused_step(FusedArgs a, int zc)
     cp_async_wait<0>();
 }
 
-// tile shape and z-chunk; chosen so the grid covers the 148 SMs several times
 constexpr int kFTX = 32, kFTY = 8;
 
-static int zchunk_for(int nx, int ny, int nz)
+// z-chunk length: every block is resident at once when the tiles fit in the
+// SMs' block slots (no partial last wave); large grids fall back to one chunk
+// per tile column and full waves.
+static int zchunk_for(int nx, int ny, int nz, int slots)
 {
     long long tiles = (long long)((nx + kFTX - 1) / kFTX) * ((ny + kFTY - 1) / kFTY);
-    long long want = 148LL * 8;
-    long long chunks = (want + tiles - 1) / tiles;
+    long long chunks = slots > 0 ? slots / tiles : 1;
     if (chunks < 1) chunks = 1;
     int zc = (int)((nz + chunks - 1) / chunks);
-    if (zc < 16) zc = 16;
+    if (zc < 8) zc = 8;
     return zc;
 }
 
 int fused_supported(int nx, int ny, int nz) { return nx >= 4 && ny >= 4 && nz >= 4; }
 
 template <bool CPML, bool LOSSY>
-static void launch_variant(const FusedArgs &a, dim3 grid, dim3 block, int zc, cudaStream_t st)
+static void launch_variant(const FusedArgs &a, cudaStream_t st)
 {
+    auto kern = k_fused_step<kFTX, kFTY, CPML, LOSSY>;
     const size_t smem = sizeof(FusedSmem<kFTX, kFTY, LOSSY>);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_fused_step<kFTX, kFTY, CPML, LOSSY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-        attr = true;
+    static int slots = -1;
+    if (slots < 0) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int per_sm = 0, dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFTX * kFTY, smem);
+        slots = per_sm * sms;
     }
-    k_fused_step<kFTX, kFTY, CPML, LOSSY><<<grid, block, smem, st>>>(a, zc);
+    const int zc = zchunk_for(a.nx, a.ny, a.nz, slots);
+    dim3 grid((a.nx + kFTX - 1) / kFTX, (a.ny + kFTY - 1) / kFTY, (a.nz + zc - 1) / zc);
+    kern<<<grid, dim3(kFTX, kFTY), smem, st>>>(a, zc);
 }
 
 void launch_fused_step(const FusedArgs &a, cudaStream_t st)
 {
-    const int zc = zchunk_for(a.nx, a.ny, a.nz);
-    dim3 grid((a.nx + kFTX - 1) / kFTX, (a.ny + kFTY - 1) / kFTY, (a.nz + zc - 1) / zc);
-    dim3 block(kFTX, kFTY);
     note_launch();
     const bool lossy = a.ca[0] != nullptr;
     if (a.L > 0) {
-        if (lossy) launch_variant<true, true>(a, grid, block, zc, st);
-        else launch_variant<true, false>(a, grid, block, zc, st);
+        if (lossy) launch_variant<true, true>(a, st);
+        else launch_variant<true, false>(a, st);
     } else {
-        if (lossy) launch_variant<false, true>(a, grid, block, zc, st);
-        else launch_variant<false, false>(a, grid, block, zc, st);
+        if (lossy) launch_variant<false, true>(a, st);
+        else launch_variant<false, false>(a, st);
     }
 }
 

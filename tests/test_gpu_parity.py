@@ -103,8 +103,13 @@ def fused_problem(lib, t, dims, lossy):
         lib.timefield3d_set_prism_electric_conductivity(t, 0.4, nx // 3, nx // 2, ny // 3, ny // 2, nz // 3, nz // 2)
 
 
-@pytest.mark.parametrize("dims,boundary,lossy", [((37, 19, 45), "cpml", False), ((64, 40, 150), "cpml", True),
-                                                  ((33, 17, 40), "pec", False)])
+@pytest.mark.parametrize("dims,boundary,lossy", [
+    ((37, 19, 45), "cpml", False),   # width not a multiple of 4: cp.async staging
+    ((33, 17, 40), "pec", False),
+    ((64, 40, 150), "cpml", True),   # TMA staging, lossy coefficients, several z-chunks
+    ((48, 24, 40), "cpml", False),   # TMA staging
+    ((72, 20, 36), "pec", False),    # TMA staging, partial edge tile
+])
 def test_fused_f32_matches_oracle(fd, orc, gpu, dims, boundary, lossy):
     """FP32 single-pass kernel (mu = 1, no magnetic loss) against the FP64 restatement."""
     nx, ny, nz = dims

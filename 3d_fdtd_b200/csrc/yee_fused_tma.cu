@@ -32,14 +32,20 @@ constexpr int EW = TX + 4;   // E / coefficient box width: x from X0 to X0+TX+3
 constexpr int HOFF = 4;      // smem x index of tile column 0 in an H box
 constexpr unsigned kWaitLimit = 1u << 22;
 
+// every TMA destination starts on a 128-byte boundary: box buffers are padded
+constexpr int pad128f(int nfloats) { return ((nfloats * 4 + 127) / 128) * 32; }
+constexpr int HBOX = (TY + 2) * HW, EBOX = (TY + 1) * EW;
+constexpr int HBOXP = pad128f(HBOX), EBOXP = pad128f(EBOX);
+
 template <bool LOSSY>
 struct alignas(128) TmaStage {
     static constexpr int NC = LOSSY ? 6 : 3;
-    float h[3][TY + 2][HW];
-    float e[3][TY + 1][EW];
-    float c[NC][TY + 1][EW];
-    static constexpr unsigned kBytes = 3u * (TY + 2) * HW * 4 + (3u + NC) * (TY + 1) * EW * 4;
+    float h[3][HBOXP];     // H box c: [TY+2][HW], x fastest
+    float e[3][EBOXP];     // E box c: [TY+1][EW]
+    float c[NC][EBOXP];    // cb (and ca) boxes
+    static constexpr unsigned kBytes = 3u * HBOX * 4 + (3u + NC) * EBOX * 4;
 };
+static_assert((HBOXP * 4) % 128 == 0 && (EBOXP * 4) % 128 == 0, "TMA box buffers must keep 128-byte alignment");
 
 template <bool LOSSY>
 struct TmaSmem {
@@ -48,6 +54,11 @@ struct TmaSmem {
     unsigned long long bar[3];
     int abort;
 };
+// dynamic shared memory requested: the struct plus room to align its base to 128 bytes
+template <bool LOSSY> constexpr size_t tma_smem_bytes() { return sizeof(TmaSmem<LOSSY>) + 128; }
+
+__device__ __forceinline__ float Hat(const float *box, int lx, int ly) { return box[(ly + 1) * HW + lx + HOFF]; }
+__device__ __forceinline__ float Eat(const float *box, int lx, int ly) { return box[ly * EW + lx]; }
 
 // ---- PTX wrappers ----------------------------------------------------------
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -102,11 +113,25 @@ __device__ __forceinline__ void issue_plane(TmaSmem<LOSSY> &sm, const FusedMaps 
     mbar_expect_tx(bar, TmaStage<LOSSY>::kBytes);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        tma_load_3d(&s.h[c][0][0], &m.h[c], X0 - HOFF, Y0 - 1, k, bar);
-        tma_load_3d(&s.e[c][0][0], &m.e[c], X0, Y0, k, bar);
-        tma_load_3d(&s.c[c][0][0], &m.cb[c], X0, Y0, k, bar);
-        if (LOSSY) tma_load_3d(&s.c[3 + c][0][0], &m.ca[c], X0, Y0, k, bar);
+        tma_load_3d(&s.h[c][0], &m.h[c], X0 - HOFF, Y0 - 1, k, bar);
+        tma_load_3d(&s.e[c][0], &m.e[c], X0, Y0, k, bar);
+        tma_load_3d(&s.c[c][0], &m.cb[c], X0, Y0, k, bar);
+        if (LOSSY) tma_load_3d(&s.c[3 + c][0], &m.ca[c], X0, Y0, k, bar);
     }
+}
+
+// true when every TMA destination is 128-byte aligned and every mbarrier 8-byte aligned
+template <bool LOSSY>
+__device__ __forceinline__ bool tma_layout_ok(const TmaSmem<LOSSY> &sm)
+{
+    for (int s = 0; s < 3; s++) {
+        for (int c = 0; c < 3; c++)
+            if ((smem_u32(&sm.st[s].h[c][0]) & 127u) || (smem_u32(&sm.st[s].e[c][0]) & 127u)) return false;
+        for (int c = 0; c < TmaStage<LOSSY>::NC; c++)
+            if (smem_u32(&sm.st[s].c[c][0]) & 127u) return false;
+        if (smem_u32(&sm.bar[s]) & 7u) return false;
+    }
+    return true;
 }
 
 template <bool LOSSY>
@@ -116,8 +141,8 @@ __device__ __forceinline__ void wait_plane(TmaSmem<LOSSY> &sm, int k, int z0, in
     const unsigned parity = (unsigned)(((k - z0 + 1) / 3) & 1);
     volatile int *abort = &sm.abort;
     for (unsigned it = 0; it < kWaitLimit; it++) {
+        if (*abort) return;   // checked first: after a refused start the barriers were never set up
         if (mbar_try_wait(&sm.bar[slot], parity)) return;
-        if (*abort) return;
     }
     *abort = 1;
     atomicExch(err, 1);
@@ -128,7 +153,9 @@ __global__ void __launch_bounds__(TX *TY)
 k_fused_tma(FusedArgs a, const __grid_constant__ FusedMaps maps, int zc, int *err)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    TmaSmem<LOSSY> &sm = *reinterpret_cast<TmaSmem<LOSSY> *>(smem_raw);
+    // align the base explicitly: TMA destinations need 128-byte alignment
+    const unsigned pad = (128u - (smem_u32(smem_raw) & 127u)) & 127u;
+    TmaSmem<LOSSY> &sm = *reinterpret_cast<TmaSmem<LOSSY> *>(smem_raw + pad);
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const long long nxy = (long long)nx * ny;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -140,12 +167,18 @@ k_fused_tma(FusedArgs a, const __grid_constant__ FusedMaps maps, int zc, int *er
     const int L = a.L;
 
     if (tid == 0) {
-        for (int s = 0; s < 3; s++) mbar_init(&sm.bar[s], 1);
-        sm.abort = 0;
+        // self-check before any copy is issued: a misaligned destination would
+        // fault, so refuse (error flag, abort) instead
+        const bool layout_ok = tma_layout_ok<LOSSY>(sm);
+        if (layout_ok)
+            for (int s = 0; s < 3; s++) mbar_init(&sm.bar[s], 1);
+        sm.abort = layout_ok ? 0 : 1;
+        if (!layout_ok) atomicExch(err, 2);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     __syncthreads();
-    if (tid == 0) {
+    const bool live = sm.abort == 0;
+    if (tid == 0 && live) {
         issue_plane<LOSSY>(sm, maps, z0 - 1, X0, Y0);
         issue_plane<LOSSY>(sm, maps, z0, X0, Y0);
     }
@@ -174,18 +207,17 @@ k_fused_tma(FusedArgs a, const __grid_constant__ FusedMaps maps, int zc, int *er
         const int ggi = X0 + lx, ggj = Y0 + ly;
         const int p3 = k % 3, pm3 = (k + 2) % 3, p2 = k & 1;
         const TmaStage<LOSSY> &S = sm.st[p3];
-        float ex = S.e[0][ly][lx], ey = S.e[1][ly][lx], ez = S.e[2][ly][lx];
+        float ex = Eat(S.e[0], lx, ly), ey = Eat(S.e[1], lx, ly), ez = Eat(S.e[2], lx, ly);
         const bool interior = ggi >= 1 && ggi <= nx - 2 && ggj >= 1 && ggj <= ny - 2 && k >= 1 && k <= nz - 2;
         if (interior) {
             const TmaStage<LOSSY> &Sm = sm.st[pm3];
-            const int hx = lx + HOFF, hy = ly + 1;
-            const float hx0 = S.h[0][hy][hx], hy0 = S.h[1][hy][hx], hz0 = S.h[2][hy][hx];
-            const float dHz_dy = hz0 - S.h[2][hy - 1][hx];
-            const float dHy_dz = hy0 - Sm.h[1][hy][hx];
-            const float dHx_dz = hx0 - Sm.h[0][hy][hx];
-            const float dHz_dx = hz0 - S.h[2][hy][hx - 1];
-            const float dHy_dx = hy0 - S.h[1][hy][hx - 1];
-            const float dHx_dy = hx0 - S.h[0][hy - 1][hx];
+            const float hx0 = Hat(S.h[0], lx, ly), hy0 = Hat(S.h[1], lx, ly), hz0 = Hat(S.h[2], lx, ly);
+            const float dHz_dy = hz0 - Hat(S.h[2], lx, ly - 1);
+            const float dHy_dz = hy0 - Hat(Sm.h[1], lx, ly);
+            const float dHx_dz = hx0 - Hat(Sm.h[0], lx, ly);
+            const float dHz_dx = hz0 - Hat(S.h[2], lx - 1, ly);
+            const float dHy_dx = hy0 - Hat(S.h[1], lx - 1, ly);
+            const float dHx_dy = hx0 - Hat(S.h[0], lx, ly - 1);
             float cx, cy, cz;
             const long long cij = ggi + (long long)nx * ggj;
             if (!CPML) {
@@ -227,13 +259,13 @@ k_fused_tma(FusedArgs a, const __grid_constant__ FusedMaps maps, int zc, int *er
                     cz -= dx * sp[2 * nxy + cij];
                 }
             if (LOSSY) {
-                ex = S.c[3][ly][lx] * ex + S.c[0][ly][lx] * cx;
-                ey = S.c[4][ly][lx] * ey + S.c[1][ly][lx] * cy;
-                ez = S.c[5][ly][lx] * ez + S.c[2][ly][lx] * cz;
+                ex = Eat(S.c[3], lx, ly) * ex + Eat(S.c[0], lx, ly) * cx;
+                ey = Eat(S.c[4], lx, ly) * ey + Eat(S.c[1], lx, ly) * cy;
+                ez = Eat(S.c[5], lx, ly) * ez + Eat(S.c[2], lx, ly) * cz;
             } else {
-                ex = ex + S.c[0][ly][lx] * cx;
-                ey = ey + S.c[1][ly][lx] * cy;
-                ez = ez + S.c[2][ly][lx] * cz;
+                ex = ex + Eat(S.c[0], lx, ly) * cx;
+                ey = ey + Eat(S.c[1], lx, ly) * cy;
+                ez = ez + Eat(S.c[2], lx, ly) * cz;
             }
             if (owned) {
                 const long long q = cij + nxy * k;
@@ -264,7 +296,7 @@ k_fused_tma(FusedArgs a, const __grid_constant__ FusedMaps maps, int zc, int *er
     };
 
     for (int k = z0; k <= z1; k++) {
-        if (tid == 0 && k + 1 <= z1 && k + 1 < nz) issue_plane<LOSSY>(sm, maps, k + 1, X0, Y0);
+        if (tid == 0 && live && k + 1 <= z1 && k + 1 < nz) issue_plane<LOSSY>(sm, maps, k + 1, X0, Y0);
         if (k < nz) {
             if (k == z0) wait_plane<LOSSY>(sm, z0 - 1, z0, err);
             wait_plane<LOSSY>(sm, k, z0, err);
@@ -329,9 +361,9 @@ k_fused_tma(FusedArgs a, const __grid_constant__ FusedMaps maps, int zc, int *er
                     cz += dx * sp[5 * nxy + ij];
                 }
             const long long q = ij + nxy * km;
-            a.f_out[3][q] = Sm.h[0][ty + 1][tx + HOFF] - hb * cx;
-            a.f_out[4][q] = Sm.h[1][ty + 1][tx + HOFF] - hb * cy;
-            a.f_out[5][q] = Sm.h[2][ty + 1][tx + HOFF] - hb * cz;
+            a.f_out[3][q] = Hat(Sm.h[0], tx, ty) - hb * cx;
+            a.f_out[4][q] = Hat(Sm.h[1], tx, ty) - hb * cy;
+            a.f_out[5][q] = Hat(Sm.h[2], tx, ty) - hb * cz;
         }
         __syncthreads();
     }
@@ -390,7 +422,7 @@ template <bool CPML, bool LOSSY>
 static void launch_tma(const FusedArgs &a, const FusedMaps &m, int *err, cudaStream_t st)
 {
     auto kern = k_fused_tma<CPML, LOSSY>;
-    const size_t smem = sizeof(TmaSmem<LOSSY>);
+    const size_t smem = tma_smem_bytes<LOSSY>();
     static int slots = -1;
     if (slots < 0) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -155,6 +155,8 @@ SIGNATURES = {
     "timefield3d_upload_materials": (i, [T]),
     "timefield3d_set_kernel_timing": (i, [T, i]),
     "timefield3d_read_kernel_timing": (i, [T, dp, C.POINTER(ll)]),
+    "fdtd_mode_overlap_plane_noalloc": (i, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, i, i, i, i, i,
+                                            C.c_void_p, i, i, d, i, d, C.c_void_p, C.c_void_p]),
 }
 
 

@@ -297,6 +297,28 @@ int timefield3d_upload_materials(timefield3d psi);
  * returns the summed milliseconds and the number of timed steps, then resets. */
 int timefield3d_set_kernel_timing(timefield3d psi, int on);
 int timefield3d_read_kernel_timing(timefield3d psi, double *total_ms, long long *count);
+
+/* Mode overlap of one z-plane that allocates nothing.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory -- code running
+ * while a stream is captured into a CUDA graph, applications that own a fixed
+ * device-memory budget, loops that cannot afford cudaMalloc's implicit
+ * synchronisation -- this computes the instantaneous overlap of
+ * timefield3d_mode_overlap (timefield3d.c:3176-3233) entirely from
+ * caller-owned device memory: ex, ey, hx, hy point to the nx*ny values of one
+ * z-plane (x fastest; double for FDTD_F64, float for FDTD_F32), mode_fields
+ * to the 6*mode_i*mode_j complex values of a power-normalised mode in the
+ * layout of mode.fields.m, result to one complex that receives
+ * -disc^2/2 * sum; ratio = disc / mode disc.  Work is queued on `stream`
+ * (a cudaStream_t, or NULL for the default stream); the call returns at once.
+ * Scratch is a fixed file-scope device array of one partial per plane row:
+ * ny may be at most 8192 (larger planes are rejected with FDTD_ERR_ARG).  The
+ * first call on each device looks the array's address up; make that first
+ * call before any stream capture.  Calls share the array, so calls that can
+ * run concurrently on the GPU race; order them on one stream. */
+int fdtd_mode_overlap_plane_noalloc(const void *ex, const void *ey, const void *hx, const void *hy, int precision,
+                                    int nx, int ny, int center_x, int center_y, const complex *mode_fields,
+                                    int mode_i, int mode_j, double ratio, int reverse, double disc,
+                                    complex *result, void *stream);
 /* copy the device edge storage into taper.forward_fields/adjoint_fields in the
  * reference layout [t][k][j][edge][6] (E components; H left zero) */
 int adjoint3d_taper_sync_host(adjoint3d_taper taper);

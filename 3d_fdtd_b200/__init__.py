@@ -25,6 +25,7 @@ FDTD_OK, FDTD_ERR_NO_DEVICE, FDTD_ERR_CUDA, FDTD_ERR_ARG, FDTD_ERR_ALLOC = 0, 1,
 FDTD_ERR_UNSUPPORTED, FDTD_ERR_TIMEOUT, FDTD_ERR_NONFINITE = 5, 6, 7
 F64, F32 = 0, 1
 MUR, CPML, PEC = 0, 1, 2
+YEE_AUTO, YEE_FLAT, YEE_FUSED = 0, 1, 2
 
 # the reference's constants (3d_fdtd.c:12, timefield3d.c:3)
 REF_PI = 3.141592652
@@ -129,6 +130,7 @@ SIGNATURES = {
     "fdtd_version": (C.c_char_p, []),
     "timefield3d_set_precision": (i, [T, i]),
     "timefield3d_set_boundary": (i, [T, i]),
+    "timefield3d_set_yee_variant": (i, [T, i]),
     "timefield3d_set_cpml": (i, [T, i, i, d, d, d]),
     "timefield3d_sync_host": (i, [T]),
     "timefield3d_sync_device": (i, [T]),

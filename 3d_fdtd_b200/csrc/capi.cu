@@ -788,6 +788,20 @@ int timefield3d_set_boundary(timefield3d psi, int boundary)
     return FDTD_OK;
 }
 
+int timefield3d_set_yee_variant(timefield3d psi, int variant)
+{
+    LOCK;
+    Grid *g = grid_lookup(psi);
+    if (!g) return FDTD_ERR_ARG;
+    if (variant < FDTD_YEE_AUTO || variant > FDTD_YEE_FUSED) {
+        set_error(FDTD_ERR_ARG, "yee variant %d", variant);
+        return FDTD_ERR_ARG;
+    }
+    g->yee_variant = variant;
+    g->version++;
+    return FDTD_OK;
+}
+
 int timefield3d_set_cpml(timefield3d psi, int thickness, int order, double sigma_max, double kappa_max, double alpha_max)
 {
     LOCK;

@@ -627,10 +627,18 @@ static bool build_profiles(Grid *g, double dt)
     return true;
 }
 
+// FP32 fast path: precomputed E coefficients, scalar H coefficient (mu = 1,
+// no magnetic loss), CPML or PEC boundary
+static bool fast32_path(const Grid *g)
+{
+    return g->prec == FDTD_F32 && g->boundary != FDTD_BOUNDARY_MUR && !g->sig_m && !g->mu_nonunit;
+}
+
+// which kernel design the fast path uses: the flat pair by default (it runs
+// at a higher fraction of HBM bandwidth on B200 than the plane-streaming kernel)
 static bool fused_path(const Grid *g)
 {
-    return g->prec == FDTD_F32 && g->boundary != FDTD_BOUNDARY_MUR && !g->sig_m && !g->mu_nonunit &&
-           fused_supported(g->nx, g->ny, g->nz);
+    return fast32_path(g) && g->yee_variant == FDTD_YEE_FUSED && fused_supported(g->nx, g->ny, g->nz);
 }
 
 // FP32 E-update coefficients of the fused path: cb = main/dx, ca = main*coef,
@@ -695,6 +703,8 @@ bool grid_prepare_step(Grid *g, double dt)
             }
             g->pp_synced = true;
         }
+    }
+    if (fast32_path(g)) {
         if (!g->coef_valid || g->coef_dt != dt) {
             size_t fb = (size_t)g->n * sizeof(float);
             for (int c = 0; c < 3; c++) {
@@ -708,11 +718,14 @@ bool grid_prepare_step(Grid *g, double dt)
             }
             g->coef_valid = true;
             g->coef_dt = dt;
-            // TMA descriptors (host-side encode; they only depend on the buffers)
             delete g->fmaps[0];
             delete g->fmaps[1];
             g->fmaps[0] = g->fmaps[1] = nullptr;
-            if (fused_tma_supported(g->nx, g->ny, g->nz)) {
+            g->version++;
+        }
+        // TMA descriptors of the fused kernel (host-side encode; they only depend on the buffers)
+        if (fused && !g->fmaps[0] && fused_tma_supported(g->nx, g->ny, g->nz)) {
+            {
                 for (int s = 0; s < 2; s++) {
                     FusedMaps *m = new FusedMaps();
                     const float *ca3[3] = {g->sig_e ? g->ca[0] : nullptr, g->sig_e ? g->ca[1] : nullptr,
@@ -819,6 +832,25 @@ template <typename T> static bool step_split(Grid *g, double dt)
     return true;
 }
 
+static bool step_flat(Grid *g, double dt)
+{
+    FlatArgs a{};
+    a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
+    for (int m = 0; m < 6; m++) a.f[m] = (float *)g->f[g->cur][m];
+    for (int c = 0; c < 3; c++) { a.cb[c] = g->cb[c]; a.ca[c] = g->sig_e ? g->ca[c] : nullptr; }
+    a.hb = (float)(dt / g->dx);
+    a.dx = (float)g->dx;
+    a.L = g->boundary == FDTD_BOUNDARY_CPML ? g->L : 0;
+    for (int ax = 0; ax < 3; ax++) {
+        for (int w = 0; w < 4; w++) a.psi[ax][w] = (float *)g->psi[g->cur][ax][w];
+        for (int w = 0; w < 6; w++) a.prof[w][ax] = (const float *)g->prof[w][ax];
+    }
+    a.src = source_table(g);
+    launch_flat_step(a, g->st, nullptr);
+    CKL("flat step");
+    return true;
+}
+
 static bool step_fused(Grid *g, double dt)
 {
     FusedArgs a{};
@@ -917,6 +949,7 @@ bool enqueue_step(Grid *g, double dt, bool with_extras)
     if (g->cap_ev) CK(cudaEventRecordWithFlags(g->cap_ev[2 * g->cap_step], g->st, cudaEventRecordExternal));
     if (g->prec == FDTD_F64) ok = step_split<double>(g, dt);
     else if (fused_path(g)) ok = step_fused(g, dt);
+    else if (fast32_path(g)) ok = step_flat(g, dt);
     else ok = step_split<float>(g, dt);
     if (!ok) return false;
     if (g->cap_ev) CK(cudaEventRecordWithFlags(g->cap_ev[2 * g->cap_step + 1], g->st, cudaEventRecordExternal));

@@ -81,6 +81,7 @@ struct Grid {
     double dx = 0;
     int prec = FDTD_F64;
     int boundary = FDTD_BOUNDARY_MUR;
+    int yee_variant = FDTD_YEE_AUTO;   // FP32 fast path: flat kernels or plane-streaming fused kernel
 
     // device state
     bool dev = false;

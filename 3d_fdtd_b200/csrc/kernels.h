@@ -59,6 +59,20 @@ struct FusedArgs {
 int fused_supported(int nx, int ny, int nz);
 void launch_fused_step(const FusedArgs &a, cudaStream_t st);
 
+// yee_flat.cu (FP32 step as two flat, one-thread-per-cell kernels, in place)
+struct FlatArgs {
+    int nx, ny, nz;
+    float *f[6];
+    const float *cb[3];
+    const float *ca[3];      // null: lossless
+    float hb, dx;
+    int L;
+    float *psi[3][4];
+    const float *prof[6][3];
+    SourcePlanes src;
+};
+void launch_flat_step(const FlatArgs &a, cudaStream_t st, cudaEvent_t mid);
+
 // yee_fused_tma.cu (the same step with TMA staging; needs nx % 4 == 0)
 struct FusedMaps {
     CUtensorMap h[3];    // H components of the input set, box (TX+8) x (TY+2)

@@ -208,7 +208,7 @@ def config_block(args) -> dict:
 class Taper:
     """One simulation of the workload on one GPU."""
 
-    def __init__(self, fd, time_steps: int):
+    def __init__(self, fd, time_steps: int, variant: int = 0):
         self.fd, self.T = fd, time_steps
         lib = fd.lib
         nx, ny, nz, dx = W["nx"], W["ny"], W["nz"], W["dx"]
@@ -217,6 +217,7 @@ class Taper:
         self.t = self.grid.t
         rasterise(lib, self.t)
         fd.call("timefield3d_set_cpml", self.t, W["cpml"], 3, -1.0, 1.0, 0.0)
+        fd.call("timefield3d_set_yee_variant", self.t, variant)
         self.mode_in = fd.read_mode_file(os.path.join(MODES, "c1_in_te0.txt.gz"))
         self.mode_out = fd.read_mode_file(os.path.join(MODES, "c1_out_te0.txt.gz"))
         self.amp, self.phase = source_tables(time_steps, self.dt)
@@ -309,7 +310,7 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    sim = Taper(fd, args.time_steps)
+    sim = Taper(fd, args.time_steps, {"auto": 0, "flat": 1, "fused": 2}[args.yee_variant])
     stream = torch.cuda.ExternalStream(fd.lib.timefield3d_get_stream(sim.t))
     cells = W["nx"] * W["ny"] * W["nz"]
     # warm-up: full runs (graph capture, clocks)
@@ -398,6 +399,7 @@ def main():
     ap.add_argument("--time-steps", type=int, default=W["time_steps"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--yee-variant", choices=["auto", "flat", "fused"], default="auto")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

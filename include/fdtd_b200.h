@@ -220,6 +220,10 @@ enum fdtd_status {
     FDTD_ERR_NONFINITE = 7      /* NaN/Inf found in materials */
 };
 enum fdtd_precision { FDTD_F64 = 0, FDTD_F32 = 1 };
+/* FP32 grids with mu = 1, no magnetic loss and a CPML or PEC boundary run one of
+ * two kernel designs: flat (one thread per cell, separate E and H launches) or
+ * fused (one launch per step streaming z-planes through shared memory). */
+enum fdtd_yee_variant { FDTD_YEE_AUTO = 0, FDTD_YEE_FLAT = 1, FDTD_YEE_FUSED = 2 };
 enum fdtd_boundary { FDTD_BOUNDARY_MUR = 0, FDTD_BOUNDARY_CPML = 1, FDTD_BOUNDARY_PEC = 2 };
 
 /* status of the last failing call on this thread (sticky until cleared) */
@@ -235,6 +239,8 @@ const char *fdtd_version(void);
  * Changing precision or boundary keeps the current fields. */
 int timefield3d_set_precision(timefield3d psi, int precision);
 int timefield3d_set_boundary(timefield3d psi, int boundary);
+/* kernel design of the FP32 fast path (enum fdtd_yee_variant); results agree to FP32 rounding */
+int timefield3d_set_yee_variant(timefield3d psi, int variant);
 /* CPML of `thickness` cells on every face, polynomial grading `order`;
  * sigma_max <= 0 selects 0.8 (order+1)/disc; kappa_max >= 1; alpha_max >= 0.
  * Profiles depend on delta_t and are rebuilt when the step size changes.

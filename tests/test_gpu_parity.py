@@ -103,19 +103,21 @@ def fused_problem(lib, t, dims, lossy):
         lib.timefield3d_set_prism_electric_conductivity(t, 0.4, nx // 3, nx // 2, ny // 3, ny // 2, nz // 3, nz // 2)
 
 
+@pytest.mark.parametrize("variant", ["flat", "fused"])
 @pytest.mark.parametrize("dims,boundary,lossy", [
-    ((37, 19, 45), "cpml", False),   # width not a multiple of 4: cp.async staging
+    ((37, 19, 45), "cpml", False),   # width not a multiple of 4: cp.async staging when fused
     ((33, 17, 40), "pec", False),
-    ((64, 40, 150), "cpml", True),   # TMA staging, lossy coefficients, several z-chunks
-    ((48, 24, 40), "cpml", False),   # TMA staging
-    ((72, 20, 36), "pec", False),    # TMA staging, partial edge tile
+    ((64, 40, 150), "cpml", True),   # TMA staging when fused, lossy coefficients, several z-chunks
+    ((48, 24, 40), "cpml", False),
+    ((72, 20, 36), "pec", False),    # partial edge tile
 ])
-def test_fused_f32_matches_oracle(fd, orc, gpu, dims, boundary, lossy):
-    """FP32 single-pass kernel (mu = 1, no magnetic loss) against the FP64 restatement."""
+def test_fused_f32_matches_oracle(fd, orc, gpu, dims, boundary, lossy, variant):
+    """FP32 fast path (mu = 1, no magnetic loss), both kernel designs, against the FP64 restatement."""
     nx, ny, nz = dims
     dx = 0.02
     dt = DT_FACTOR * dx
     grid = fd.Grid(nx, ny, nz, dx, fd.F32)
+    fd.call("timefield3d_set_yee_variant", grid.t, fd.YEE_FLAT if variant == "flat" else fd.YEE_FUSED)
     fused_problem(fd.lib, grid.t, dims, lossy)
     g = oracle_copy(orc, grid)
     if boundary == "cpml":
@@ -139,7 +141,8 @@ def test_fused_f32_matches_oracle(fd, orc, gpu, dims, boundary, lossy):
         launches.append(fd.lib.fdtd_launch_count() - l0)
         g.step(dt)
     fd.check("fused loop")
-    assert max(launches[5:]) == 2          # one Yee kernel + the step counter
+    # Yee kernels (2 flat, 1 fused) + the step counter
+    assert max(launches[5:]) == (3 if variant == "flat" else 2)
     a, b = grid.fields(), g.fields()
     err = np.abs(a - b).max() / np.abs(b).max()
     assert np.abs(b).max() > 1e-3

@@ -25,7 +25,7 @@ FDTD_OK, FDTD_ERR_NO_DEVICE, FDTD_ERR_CUDA, FDTD_ERR_ARG, FDTD_ERR_ALLOC = 0, 1,
 FDTD_ERR_UNSUPPORTED, FDTD_ERR_TIMEOUT, FDTD_ERR_NONFINITE = 5, 6, 7
 F64, F32 = 0, 1
 MUR, CPML, PEC = 0, 1, 2
-YEE_AUTO, YEE_FLAT, YEE_FUSED = 0, 1, 2
+YEE_AUTO, YEE_FLAT, YEE_FUSED, YEE_FLAT4 = 0, 1, 2, 3
 
 # the reference's constants (3d_fdtd.c:12, timefield3d.c:3)
 REF_PI = 3.141592652

@@ -793,7 +793,7 @@ int timefield3d_set_yee_variant(timefield3d psi, int variant)
     LOCK;
     Grid *g = grid_lookup(psi);
     if (!g) return FDTD_ERR_ARG;
-    if (variant < FDTD_YEE_AUTO || variant > FDTD_YEE_FUSED) {
+    if (variant < FDTD_YEE_AUTO || variant > FDTD_YEE_FLAT4) {
         set_error(FDTD_ERR_ARG, "yee variant %d", variant);
         return FDTD_ERR_ARG;
     }

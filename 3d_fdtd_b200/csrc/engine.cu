@@ -355,6 +355,10 @@ Grid::~Grid()
         for (auto &kv : d_dft_slice) dfree(kv.second);
         if (sched.active) { dfree(sched.d_sched); priv_mode_free(sched.mode_key); }
         dfree(d_aos);
+        cudaStreamSynchronize(side);
+        cudaEventDestroy(ev_fork);
+        cudaEventDestroy(ev_join);
+        cudaStreamDestroy(side);
         cudaStreamDestroy(st);
     }
 }
@@ -519,6 +523,9 @@ bool grid_ensure_device(Grid *g)
             return false;
         }
         CK(cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming));
         g->dev = true;
         size_t fb = (size_t)g->n * sizeof(float);
         for (int c = 0; c < 3; c++) {
@@ -846,7 +853,9 @@ static bool step_flat(Grid *g, double dt)
         for (int w = 0; w < 6; w++) a.prof[w][ax] = (const float *)g->prof[w][ax];
     }
     a.src = source_table(g);
-    launch_flat_step(a, g->st, nullptr);
+    const bool four = g->yee_variant != FDTD_YEE_FLAT && flat4_supported(g->nx, g->nz);
+    if (four) launch_flat4_step(a, g->st, g->side, g->ev_fork, g->ev_join);
+    else launch_flat_step(a, g->st, nullptr);
     CKL("flat step");
     return true;
 }

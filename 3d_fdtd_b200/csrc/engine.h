@@ -86,6 +86,8 @@ struct Grid {
     // device state
     bool dev = false;
     cudaStream_t st = nullptr;
+    cudaStream_t side = nullptr;      // second stream of the flat4 CPML shell kernels
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     void *f[2][6] = {};       // field sets; set 1 is the ping-pong buffer of the fused path
     int cur = 0;
     void *old[6] = {};        // Mur snapshot

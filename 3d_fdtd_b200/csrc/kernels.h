@@ -72,6 +72,19 @@ struct FlatArgs {
     SourcePlanes src;
 };
 void launch_flat_step(const FlatArgs &a, cudaStream_t st, cudaEvent_t mid);
+int flat4_supported(int nx, int nz);
+// cells of one flat4 launch: planes kA..kA+nA-1 then kB.., `count` (group, row)
+// slots per plane laid out by region kind (0 whole planes, 1 interior box
+// [gL, gR) x [L, ny-L), 2 the ring of y-slab rows and x-slab groups around it)
+struct Region4 {
+    int kA, nA, kB;
+    int count;
+    int gL, gR, L;
+};
+bool flat4_split_supported(const FlatArgs &a);
+// E then H update.  With a CPML and a side stream the interior box runs on `st`
+// and the shell on `side` (fork/join through the two events) for each field.
+void launch_flat4_step(const FlatArgs &a, cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join);
 
 // yee_fused_tma.cu (the same step with TMA staging; needs nx % 4 == 0)
 struct FusedMaps {

@@ -1,0 +1,522 @@
+// yee_flat4.cu -- the flat FP32 E and H kernels, W consecutive x cells per thread.
+//
+// Same arithmetic as yee_flat.cu.  A thread owns W (4 or 2) consecutive x cells
+// of one row and moves every array with W-float vector loads and stores.  Each
+// kernel runs in three phases: every load the thread needs (fields, neighbours,
+// coefficients, source plane, CPML auxiliaries and profiles) is issued first,
+// then the arithmetic, then every store.  Issuing the auxiliaries after the
+// first stores would chain a DRAM round trip per dependent load-store pair (the
+// compiler cannot prove the arrays apart), and almost every warp of a CPML
+// grid holds some x-slab cells; with the loads up front each warp waits for
+// memory once.
+//
+// The x-neighbour (i-1 for E, i+1 for H) comes from the adjacent lane by a warp
+// shuffle when that lane holds the neighbouring group of the same row, else
+// from one scalar load.  Needs nx % 4 == 0 (rows start on 16-byte boundaries);
+// other widths use yee_flat.cu.
+//
+// Regions.  Threads are laid out per z-plane over (group, row) slots.  A grid
+// without CPML runs whole planes k = 1..nz-2 with W = 4 (kind 0).  With a CPML
+// the slab instantiation holds far more state (auxiliaries, profiles), yet
+// inside the box [L, N-L) of every axis it computes exactly what the plain
+// instantiation computes (kappa = 1, auxiliaries 0).  So a CPML grid launches
+// the plain W = 4 kernel over that interior box (kind 1) and the CPML kernel
+// with W = 2, half the per-thread state and so twice the resident warps, over
+// the shell around it: the z-slab planes whole (kind 0) and, in the middle
+// planes, the ring of y-slab rows plus the x-slab groups of the other rows
+// (kind 2).  The shell runs on a second stream beside the box.
+//
+// CPML auxiliaries: the y- and z-slab ones are contiguous in x and move as
+// vectors; the x-slab ones (the groups at each end of a row) per element.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace fdtd {
+
+constexpr int kBlock4 = 256;
+
+template <int W> struct Vf { float v[W]; };
+
+template <int W> __device__ __forceinline__ Vf<W> ldv(const float *p)
+{
+    Vf<W> r;
+    if constexpr (W == 4) {
+        const float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+        r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
+    } else {
+        const float2 t = __ldg(reinterpret_cast<const float2 *>(p));
+        r.v[0] = t.x; r.v[1] = t.y;
+    }
+    return r;
+}
+
+template <int W> __device__ __forceinline__ Vf<W> ldv_rw(const float *p)
+{
+    Vf<W> r;
+    if constexpr (W == 4) {
+        const float4 t = *reinterpret_cast<const float4 *>(p);
+        r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
+    } else {
+        const float2 t = *reinterpret_cast<const float2 *>(p);
+        r.v[0] = t.x; r.v[1] = t.y;
+    }
+    return r;
+}
+
+template <int W> __device__ __forceinline__ void stv(float *p, const Vf<W> &x)
+{
+    if constexpr (W == 4) *reinterpret_cast<float4 *>(p) = make_float4(x.v[0], x.v[1], x.v[2], x.v[3]);
+    else *reinterpret_cast<float2 *>(p) = make_float2(x.v[0], x.v[1]);
+}
+
+template <int W> __device__ __forceinline__ Vf<W> fillv(float s)
+{
+    Vf<W> r;
+#pragma unroll
+    for (int e = 0; e < W; e++) r.v[e] = s;
+    return r;
+}
+
+__device__ __forceinline__ const float *src_plane(const SourcePlanes &s, int k)
+{
+    for (int t = 0; t < s.n; t++)
+        if (s.k[t] == k) return s.p[t];
+    return nullptr;
+}
+
+// x-slab state of one group: per element the CPML profile (b, a, kappa) and the
+// two auxiliaries of this field; valid[e] marks interior cells inside the slab.
+template <int W> struct XSlab {
+    bool any;
+    bool valid[W];
+    float b[W], c[W], k[W], p0[W], p1[W];
+    long long s0;  // auxiliary row base: element i sits at s0 + slab_local(i)
+};
+
+// A0 = 0 for E (auxiliaries 0, 1; profiles 0..2), 2 for H (auxiliaries 2, 3; profiles 3..5)
+template <int W, int A0>
+__device__ __forceinline__ void xslab_load(XSlab<W> &x, const FlatArgs &a, int g, int j, int k)
+{
+    const int nx = a.nx, L = a.L;
+    const int i0 = W * g;
+    constexpr int pw = A0 == 0 ? 0 : 3;
+    x.any = i0 < L || i0 + W - 1 >= nx - L;
+    x.s0 = 2LL * L * (j + (long long)a.ny * k);
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+        const int i = i0 + e;
+        const int si = slab_local(i, nx, L);
+        x.valid[e] = x.any && si >= 0 && i >= 1 && i <= nx - 2;
+        x.b[e] = 0.f; x.c[e] = 0.f; x.k[e] = 1.f; x.p0[e] = 0.f; x.p1[e] = 0.f;
+        if (x.valid[e]) {
+            const long long s = x.s0 + si;
+            x.b[e] = __ldg(a.prof[pw + 0][0] + i);
+            x.c[e] = __ldg(a.prof[pw + 1][0] + i);
+            x.k[e] = __ldg(a.prof[pw + 2][0] + i);
+            x.p0[e] = a.psi[0][A0][s];
+            x.p1[e] = a.psi[0][A0 + 1][s];
+        }
+    }
+}
+
+template <int W, int A0>
+__device__ __forceinline__ void xslab_store(const XSlab<W> &x, const FlatArgs &a, int g)
+{
+    if (!x.any) return;
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+        if (!x.valid[e]) continue;
+        const long long s = x.s0 + slab_local(W * g + e, a.nx, a.L);
+        a.psi[0][A0][s] = x.p0[e];
+        a.psi[0][A0 + 1][s] = x.p1[e];
+    }
+}
+
+// y- and z-slab state of one group (auxiliaries contiguous in x)
+template <int W> struct YZSlab {
+    int sj, sk;
+    float by, ay, ky, bz, az, kz;
+    Vf<W> pxy, pzy, pxz, pyz;  // E: (x,y) (z,y) (x,z) (y,z); H alike with auxiliaries 2, 3
+    long long sy, sz;
+};
+
+template <int W, int A0>
+__device__ __forceinline__ void yzslab_load(YZSlab<W> &s, const FlatArgs &a, int g, int j, int k, long long ij0,
+                                            long long nxy)
+{
+    const int L = a.L;
+    constexpr int pw = A0 == 0 ? 0 : 3;
+    s.sj = slab_local(j, a.ny, L);
+    s.sk = slab_local(k, a.nz, L);
+    s.by = 1.f; s.ay = 0.f; s.ky = 1.f; s.bz = 1.f; s.az = 0.f; s.kz = 1.f;
+    s.pxy = fillv<W>(0.f); s.pzy = s.pxy; s.pxz = s.pxy; s.pyz = s.pxy;
+    s.sy = 0; s.sz = 0;
+    if (s.sj >= 0) {
+        s.by = __ldg(a.prof[pw + 0][1] + j); s.ay = __ldg(a.prof[pw + 1][1] + j); s.ky = __ldg(a.prof[pw + 2][1] + j);
+        s.sy = (long long)W * g + (long long)a.nx * (s.sj + 2LL * L * k);
+        s.pxy = ldv_rw<W>(a.psi[1][A0] + s.sy);
+        s.pzy = ldv_rw<W>(a.psi[1][A0 + 1] + s.sy);
+    }
+    if (s.sk >= 0) {
+        s.bz = __ldg(a.prof[pw + 0][2] + k); s.az = __ldg(a.prof[pw + 1][2] + k); s.kz = __ldg(a.prof[pw + 2][2] + k);
+        s.sz = ij0 + nxy * s.sk;
+        s.pxz = ldv_rw<W>(a.psi[2][A0] + s.sz);
+        s.pyz = ldv_rw<W>(a.psi[2][A0 + 1] + s.sz);
+    }
+}
+
+template <int W, int A0>
+__device__ __forceinline__ void yzslab_store(const YZSlab<W> &s, const FlatArgs &a)
+{
+    if (s.sj >= 0) {
+        stv<W>(a.psi[1][A0] + s.sy, s.pxy);
+        stv<W>(a.psi[1][A0 + 1] + s.sy, s.pzy);
+    }
+    if (s.sk >= 0) {
+        stv<W>(a.psi[2][A0] + s.sz, s.pxz);
+        stv<W>(a.psi[2][A0 + 1] + s.sz, s.pyz);
+    }
+}
+
+// One cell's curl with the CPML terms.  d1, d2: the two differences of the
+// component (e.g. dHz/dy, dHy/dz for x); the auxiliaries update in place.
+struct Curl3 { float x, y, z; };
+
+template <int W>
+__device__ __forceinline__ Curl3 cpml_curl(XSlab<W> &xs, YZSlab<W> &s, int e, float d_zy, float d_yz, float d_xz,
+                                           float d_zx, float d_yx, float d_xy, float dx, float div)
+{
+    // d_ab = difference of component a along axis b
+    float pyx = 0.f, pzx = 0.f;
+    if (xs.valid[e]) {
+        pyx = xs.b[e] * xs.p0[e] + xs.c[e] * (d_zx * div);
+        pzx = xs.b[e] * xs.p1[e] + xs.c[e] * (d_yx * div);
+        xs.p0[e] = pyx;
+        xs.p1[e] = pzx;
+    }
+    float vxy = 0.f, vzy = 0.f, vxz = 0.f, vyz = 0.f;
+    if (s.sj >= 0) {
+        vxy = s.by * s.pxy.v[e] + s.ay * (d_zy * div);
+        vzy = s.by * s.pzy.v[e] + s.ay * (d_xy * div);
+        s.pxy.v[e] = vxy;
+        s.pzy.v[e] = vzy;
+    }
+    if (s.sk >= 0) {
+        vxz = s.bz * s.pxz.v[e] + s.az * (d_yz * div);
+        vyz = s.bz * s.pyz.v[e] + s.az * (d_xz * div);
+        s.pxz.v[e] = vxz;
+        s.pyz.v[e] = vyz;
+    }
+    const float kx = xs.k[e];
+    Curl3 c;
+    c.x = s.ky * d_zy - s.kz * d_yz + dx * (vxy - vxz);
+    c.y = s.kz * d_xz - kx * d_zx + dx * (vyz - pyx);
+    c.z = kx * d_yx - s.ky * d_xy + dx * (pzx - vzy);
+    return c;
+}
+
+// slot -> (group, row) of one region, and the plane of blockIdx.y
+template <int KIND>
+__device__ __forceinline__ void locate(const Region4 &r, int ngroups, int ny, int &g, int &j, int &k, bool &live)
+{
+    int s = blockIdx.x * kBlock4 + threadIdx.x;
+    const int by = blockIdx.y;
+    k = by < r.nA ? r.kA + by : r.kB + (by - r.nA);
+    live = s < r.count;
+    if (KIND == 0) {
+        g = s % ngroups;
+        j = s / ngroups;
+        live = live && j >= 1 && j <= ny - 2;
+    } else if (KIND == 1) {
+        const int gw = r.gR - r.gL;
+        g = r.gL + s % gw;
+        j = r.L + s / gw;
+    } else {
+        const int band = (r.L - 1) * ngroups;
+        if (s < band) {
+            g = s % ngroups;
+            j = 1 + s / ngroups;
+        } else if (s < 2 * band) {
+            s -= band;
+            g = s % ngroups;
+            j = ny - r.L + s / ngroups;
+        } else {
+            s -= 2 * band;
+            const int w = r.gL + ngroups - r.gR;
+            const int rr = s % w;
+            j = r.L + s / w;
+            g = rr < r.gL ? rr : r.gR + (rr - r.gL);
+        }
+    }
+}
+
+template <int W, bool CPML, bool LOSSY, int KIND>
+__global__ void __launch_bounds__(kBlock4, W == 4 ? 2 : 3) k_flat4_E(FlatArgs a, Region4 r)
+{
+    const int nx = a.nx, ny = a.ny;
+    const int ngroups = nx / W;
+    const int lane = threadIdx.x & 31;
+    int g, j, k;
+    bool live;
+    locate<KIND>(r, ngroups, ny, g, j, k, live);
+    const long long nxy = (long long)nx * ny;
+    const long long ij0 = (long long)W * g + (long long)nx * j;
+    const long long q0 = ij0 + nxy * k;
+    // neighbour lanes hold the adjacent group of the same row when their keys are adjacent
+    const int key = live ? j * ngroups + g : -2;
+    // ---- phase 1: loads
+    Vf<W> hy = fillv<W>(0.f), hz = hy;
+    if (live) {
+        hy = ldv<W>(a.f[4] + q0);
+        hz = ldv<W>(a.f[5] + q0);
+    }
+    // the i-1 neighbour of element 0 is lane-1's last element when lane-1 holds group g-1
+    float hy_im0 = __shfl_up_sync(0xffffffffu, hy.v[W - 1], 1);
+    float hz_im0 = __shfl_up_sync(0xffffffffu, hz.v[W - 1], 1);
+    const int key_prev = __shfl_up_sync(0xffffffffu, key, 1);
+    if (!live) return;
+    if (lane == 0 || g == 0 || key_prev != key - 1) {
+        hy_im0 = g > 0 ? __ldg(a.f[4] + q0 - 1) : 0.f;
+        hz_im0 = g > 0 ? __ldg(a.f[5] + q0 - 1) : 0.f;
+    }
+    const Vf<W> hx = ldv<W>(a.f[3] + q0);
+    const Vf<W> hx_jm = ldv<W>(a.f[3] + q0 - nx), hz_jm = ldv<W>(a.f[5] + q0 - nx);
+    const Vf<W> hx_km = ldv<W>(a.f[3] + q0 - nxy), hy_km = ldv<W>(a.f[4] + q0 - nxy);
+    const Vf<W> b0 = ldv<W>(a.cb[0] + q0), b1 = ldv<W>(a.cb[1] + q0), b2 = ldv<W>(a.cb[2] + q0);
+    Vf<W> ex = ldv_rw<W>(a.f[0] + q0), ey = ldv_rw<W>(a.f[1] + q0), ez = ldv_rw<W>(a.f[2] + q0);
+    Vf<W> c0 = fillv<W>(1.f), c1 = c0, c2 = c0;
+    if (LOSSY) {
+        c0 = ldv<W>(a.ca[0] + q0);
+        c1 = ldv<W>(a.ca[1] + q0);
+        c2 = ldv<W>(a.ca[2] + q0);
+    }
+    const float *sp = a.src.n ? src_plane(a.src, k) : nullptr;
+    Vf<W> j0 = fillv<W>(0.f), j1 = j0, j2 = j0;
+    if (sp) {
+        j0 = ldv<W>(sp + ij0);
+        j1 = ldv<W>(sp + nxy + ij0);
+        j2 = ldv<W>(sp + 2 * nxy + ij0);
+    }
+    XSlab<W> xs;
+    YZSlab<W> ys;
+    if (CPML) {
+        yzslab_load<W, 0>(ys, a, g, j, k, ij0, nxy);
+        xslab_load<W, 0>(xs, a, g, j, k);
+    }
+    // ---- phase 2: arithmetic
+    const float dx = a.dx, div = 1.0f / dx;
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+        const int i = W * g + e;
+        if (i < 1 || i > nx - 2) continue;  // x = 0 and x = nx-1 stay
+        const float hy_im = e == 0 ? hy_im0 : hy.v[e - 1];
+        const float hz_im = e == 0 ? hz_im0 : hz.v[e - 1];
+        const float dHz_dy = hz.v[e] - hz_jm.v[e];
+        const float dHy_dz = hy.v[e] - hy_km.v[e];
+        const float dHx_dz = hx.v[e] - hx_km.v[e];
+        const float dHz_dx = hz.v[e] - hz_im;
+        const float dHy_dx = hy.v[e] - hy_im;
+        const float dHx_dy = hx.v[e] - hx_jm.v[e];
+        float cx, cy, cz;
+        if (!CPML) {
+            cx = dHz_dy - dHy_dz;
+            cy = dHx_dz - dHz_dx;
+            cz = dHy_dx - dHx_dy;
+        } else {
+            const Curl3 c = cpml_curl<W>(xs, ys, e, dHz_dy, dHy_dz, dHx_dz, dHz_dx, dHy_dx, dHx_dy, dx, div);
+            cx = c.x; cy = c.y; cz = c.z;
+        }
+        if (sp) {
+            cx -= dx * j0.v[e];
+            cy -= dx * j1.v[e];
+            cz -= dx * j2.v[e];
+        }
+        ex.v[e] = c0.v[e] * ex.v[e] + b0.v[e] * cx;
+        ey.v[e] = c1.v[e] * ey.v[e] + b1.v[e] * cy;
+        ez.v[e] = c2.v[e] * ez.v[e] + b2.v[e] * cz;
+    }
+    // ---- phase 3: stores
+    stv<W>(a.f[0] + q0, ex);
+    stv<W>(a.f[1] + q0, ey);
+    stv<W>(a.f[2] + q0, ez);
+    if (CPML) {
+        yzslab_store<W, 0>(ys, a);
+        xslab_store<W, 0>(xs, a, g);
+    }
+}
+
+template <int W, bool CPML, int KIND>
+__global__ void __launch_bounds__(kBlock4, W == 4 ? 2 : 3) k_flat4_H(FlatArgs a, Region4 r)
+{
+    const int nx = a.nx, ny = a.ny;
+    const int ngroups = nx / W;
+    const int lane = threadIdx.x & 31;
+    int g, j, k;
+    bool live;
+    locate<KIND>(r, ngroups, ny, g, j, k, live);
+    const long long nxy = (long long)nx * ny;
+    const long long ij0 = (long long)W * g + (long long)nx * j;
+    const long long q0 = ij0 + nxy * k;
+    const int key = live ? j * ngroups + g : -2;
+    // ---- phase 1: loads
+    Vf<W> ey = fillv<W>(0.f), ez = ey;
+    if (live) {
+        ey = ldv<W>(a.f[1] + q0);
+        ez = ldv<W>(a.f[2] + q0);
+    }
+    // the i+1 neighbour of the last element is lane+1's element 0 when lane+1 holds group g+1
+    float ey_ipw = __shfl_down_sync(0xffffffffu, ey.v[0], 1);
+    float ez_ipw = __shfl_down_sync(0xffffffffu, ez.v[0], 1);
+    const int key_next = __shfl_down_sync(0xffffffffu, key, 1);
+    if (!live) return;
+    if (lane == 31 || g == ngroups - 1 || key_next != key + 1) {
+        ey_ipw = g < ngroups - 1 ? __ldg(a.f[1] + q0 + W) : 0.f;
+        ez_ipw = g < ngroups - 1 ? __ldg(a.f[2] + q0 + W) : 0.f;
+    }
+    const Vf<W> ex = ldv<W>(a.f[0] + q0);
+    const Vf<W> ex_jp = ldv<W>(a.f[0] + q0 + nx), ez_jp = ldv<W>(a.f[2] + q0 + nx);
+    const Vf<W> ex_kp = ldv<W>(a.f[0] + q0 + nxy), ey_kp = ldv<W>(a.f[1] + q0 + nxy);
+    Vf<W> hx = ldv_rw<W>(a.f[3] + q0), hy = ldv_rw<W>(a.f[4] + q0), hz = ldv_rw<W>(a.f[5] + q0);
+    const float *sp = a.src.n ? src_plane(a.src, k) : nullptr;
+    Vf<W> m0 = fillv<W>(0.f), m1 = m0, m2 = m0;
+    if (sp) {
+        m0 = ldv<W>(sp + 3 * nxy + ij0);
+        m1 = ldv<W>(sp + 4 * nxy + ij0);
+        m2 = ldv<W>(sp + 5 * nxy + ij0);
+    }
+    XSlab<W> xs;
+    YZSlab<W> ys;
+    if (CPML) {
+        yzslab_load<W, 2>(ys, a, g, j, k, ij0, nxy);
+        xslab_load<W, 2>(xs, a, g, j, k);
+    }
+    // ---- phase 2: arithmetic
+    const float dx = a.dx, hb = a.hb, div = 1.0f / dx;
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+        const int i = W * g + e;
+        if (i < 1 || i > nx - 2) continue;
+        const float ey_ip = e == W - 1 ? ey_ipw : ey.v[e + 1];
+        const float ez_ip = e == W - 1 ? ez_ipw : ez.v[e + 1];
+        const float dEz_dy = ez_jp.v[e] - ez.v[e];
+        const float dEy_dz = ey_kp.v[e] - ey.v[e];
+        const float dEx_dz = ex_kp.v[e] - ex.v[e];
+        const float dEz_dx = ez_ip - ez.v[e];
+        const float dEy_dx = ey_ip - ey.v[e];
+        const float dEx_dy = ex_jp.v[e] - ex.v[e];
+        float cx, cy, cz;
+        if (!CPML) {
+            cx = dEz_dy - dEy_dz;
+            cy = dEx_dz - dEz_dx;
+            cz = dEy_dx - dEx_dy;
+        } else {
+            const Curl3 c = cpml_curl<W>(xs, ys, e, dEz_dy, dEy_dz, dEx_dz, dEz_dx, dEy_dx, dEx_dy, dx, div);
+            cx = c.x; cy = c.y; cz = c.z;
+        }
+        if (sp) {
+            cx += dx * m0.v[e];
+            cy += dx * m1.v[e];
+            cz += dx * m2.v[e];
+        }
+        hx.v[e] = hx.v[e] - hb * cx;
+        hy.v[e] = hy.v[e] - hb * cy;
+        hz.v[e] = hz.v[e] - hb * cz;
+    }
+    // ---- phase 3: stores
+    stv<W>(a.f[3] + q0, hx);
+    stv<W>(a.f[4] + q0, hy);
+    stv<W>(a.f[5] + q0, hz);
+    if (CPML) {
+        yzslab_store<W, 2>(ys, a);
+        xslab_store<W, 2>(xs, a, g);
+    }
+}
+
+int flat4_supported(int nx, int nz) { return nx % 4 == 0 && nx >= 8 && nz >= 3; }
+
+static Region4 planes_region(int kA, int nA, int kB, int count)
+{
+    Region4 r{};
+    r.kA = kA; r.nA = nA; r.kB = kB; r.count = count;
+    return r;
+}
+
+// kernel instantiations per launch: kind 1 -> plain W=4 box; kind 2 -> CPML W=2 ring;
+// kind 0 -> CPML W=2 z-slab planes, or plain W=4 whole planes of a grid without CPML
+template <bool LOSSY>
+static void launch_E(const FlatArgs &a, const Region4 &r, dim3 grid, int kind, bool cpml, cudaStream_t st)
+{
+    if (kind == 1) k_flat4_E<4, false, LOSSY, 1><<<grid, kBlock4, 0, st>>>(a, r);
+    else if (kind == 2) k_flat4_E<2, true, LOSSY, 2><<<grid, kBlock4, 0, st>>>(a, r);
+    else if (cpml) k_flat4_E<2, true, LOSSY, 0><<<grid, kBlock4, 0, st>>>(a, r);
+    else k_flat4_E<4, false, LOSSY, 0><<<grid, kBlock4, 0, st>>>(a, r);
+}
+
+static void launch_H(const FlatArgs &a, const Region4 &r, dim3 grid, int kind, bool cpml, cudaStream_t st)
+{
+    if (kind == 1) k_flat4_H<4, false, 1><<<grid, kBlock4, 0, st>>>(a, r);
+    else if (kind == 2) k_flat4_H<2, true, 2><<<grid, kBlock4, 0, st>>>(a, r);
+    else if (cpml) k_flat4_H<2, true, 0><<<grid, kBlock4, 0, st>>>(a, r);
+    else k_flat4_H<4, false, 0><<<grid, kBlock4, 0, st>>>(a, r);
+}
+
+static void launch_phase(bool e_phase, const FlatArgs &a, const Region4 &r, int nplanes, int kind, bool cpml,
+                         cudaStream_t st)
+{
+    if (r.count <= 0 || nplanes <= 0) return;
+    note_launch(1);
+    const dim3 grid((r.count + kBlock4 - 1) / kBlock4, nplanes);
+    if (!e_phase) launch_H(a, r, grid, kind, cpml, st);
+    else if (a.ca[0]) launch_E<true>(a, r, grid, kind, cpml, st);
+    else launch_E<false>(a, r, grid, kind, cpml, st);
+}
+
+bool flat4_split_supported(const FlatArgs &a)
+{
+    const int L = a.L;
+    if (L < 2 || a.ny <= 2 * L || a.nz <= 2 * L) return false;
+    const int gL = (L + 3) / 4, gR = (a.nx - L) / 4;
+    return gR > gL;
+}
+
+void launch_flat4_step(const FlatArgs &a, cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join)
+{
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const bool cpml = a.L > 0;
+    if (!cpml) {
+        const Region4 r = planes_region(1, nz - 2, 0, (nx / 4) * ny);
+        launch_phase(true, a, r, nz - 2, 0, false, st);
+        launch_phase(false, a, r, nz - 2, 0, false, st);
+        return;
+    }
+    if (!side || !flat4_split_supported(a)) {
+        // CPML kernel (W = 2) over whole planes
+        const Region4 r = planes_region(1, nz - 2, 0, (nx / 2) * ny);
+        launch_phase(true, a, r, nz - 2, 0, true, st);
+        launch_phase(false, a, r, nz - 2, 0, true, st);
+        return;
+    }
+    const int L = a.L, ng2 = nx / 2;
+    // interior box in 4-cell groups [gL, gR): every cell of it lies in [L, nx-L)
+    const int gL = (L + 3) / 4, gR = (nx - L) / 4;
+    Region4 box = planes_region(L, nz - 2 * L, 0, (gR - gL) * (ny - 2 * L));
+    box.gL = gL; box.gR = gR; box.L = L;
+    // shell in 2-cell groups: z-slab planes 1..L-1 and nz-L..nz-2 whole, and in
+    // the middle planes the ring around the box (its groups [2 gL, 2 gR) excluded)
+    const Region4 zs = planes_region(1, L - 1, nz - L, ng2 * ny);
+    Region4 ring = planes_region(L, nz - 2 * L, 0,
+                                 2 * (L - 1) * ng2 + (ny - 2 * L) * (2 * gL + ng2 - 2 * gR));
+    ring.gL = 2 * gL; ring.gR = 2 * gR; ring.L = L;
+    for (int phase = 0; phase < 2; phase++) {
+        const bool e = phase == 0;
+        cudaEventRecord(fork, st);
+        cudaStreamWaitEvent(side, fork, 0);
+        launch_phase(e, a, zs, 2 * (L - 1), 0, true, side);
+        launch_phase(e, a, ring, nz - 2 * L, 2, true, side);
+        launch_phase(e, a, box, nz - 2 * L, 1, false, st);
+        cudaEventRecord(join, side);
+        cudaStreamWaitEvent(st, join, 0);
+    }
+}
+
+}  // namespace fdtd

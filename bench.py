@@ -310,7 +310,7 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    sim = Taper(fd, args.time_steps, {"auto": 0, "flat": 1, "fused": 2}[args.yee_variant])
+    sim = Taper(fd, args.time_steps, {"auto": 0, "flat": 1, "fused": 2, "flat4": 3}[args.yee_variant])
     stream = torch.cuda.ExternalStream(fd.lib.timefield3d_get_stream(sim.t))
     cells = W["nx"] * W["ny"] * W["nz"]
     # warm-up: full runs (graph capture, clocks)
@@ -399,7 +399,7 @@ def main():
     ap.add_argument("--time-steps", type=int, default=W["time_steps"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--yee-variant", choices=["auto", "flat", "fused"], default="auto")
+    ap.add_argument("--yee-variant", choices=["auto", "flat", "flat4", "fused"], default="auto")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -221,9 +221,11 @@ enum fdtd_status {
 };
 enum fdtd_precision { FDTD_F64 = 0, FDTD_F32 = 1 };
 /* FP32 grids with mu = 1, no magnetic loss and a CPML or PEC boundary run one of
- * two kernel designs: flat (one thread per cell, separate E and H launches) or
- * fused (one launch per step streaming z-planes through shared memory). */
-enum fdtd_yee_variant { FDTD_YEE_AUTO = 0, FDTD_YEE_FLAT = 1, FDTD_YEE_FUSED = 2 };
+ * three kernel designs: flat (one thread per cell, separate E and H launches),
+ * flat4 (separate E and H launches, four x cells per thread with 16-byte
+ * accesses; nx % 4 == 0) or fused (one launch per step streaming z-planes through
+ * shared memory).  AUTO picks flat4 where nx allows, else flat. */
+enum fdtd_yee_variant { FDTD_YEE_AUTO = 0, FDTD_YEE_FLAT = 1, FDTD_YEE_FUSED = 2, FDTD_YEE_FLAT4 = 3 };
 enum fdtd_boundary { FDTD_BOUNDARY_MUR = 0, FDTD_BOUNDARY_CPML = 1, FDTD_BOUNDARY_PEC = 2 };
 
 /* status of the last failing call on this thread (sticky until cleared) */

@@ -103,13 +103,14 @@ def fused_problem(lib, t, dims, lossy):
         lib.timefield3d_set_prism_electric_conductivity(t, 0.4, nx // 3, nx // 2, ny // 3, ny // 2, nz // 3, nz // 2)
 
 
-@pytest.mark.parametrize("variant", ["flat", "fused"])
+@pytest.mark.parametrize("variant", ["flat", "flat4", "fused"])
 @pytest.mark.parametrize("dims,boundary,lossy", [
     ((37, 19, 45), "cpml", False),   # width not a multiple of 4: cp.async staging when fused
     ((33, 17, 40), "pec", False),
     ((64, 40, 150), "cpml", True),   # TMA staging when fused, lossy coefficients, several z-chunks
     ((48, 24, 40), "cpml", False),
     ((72, 20, 36), "pec", False),    # partial edge tile
+    ((36, 21, 30), "cpml", True),    # nine 4-cell groups per row: rows start inside a warp
 ])
 def test_fused_f32_matches_oracle(fd, orc, gpu, dims, boundary, lossy, variant):
     """FP32 fast path (mu = 1, no magnetic loss), both kernel designs, against the FP64 restatement."""
@@ -117,7 +118,8 @@ def test_fused_f32_matches_oracle(fd, orc, gpu, dims, boundary, lossy, variant):
     dx = 0.02
     dt = DT_FACTOR * dx
     grid = fd.Grid(nx, ny, nz, dx, fd.F32)
-    fd.call("timefield3d_set_yee_variant", grid.t, fd.YEE_FLAT if variant == "flat" else fd.YEE_FUSED)
+    fd.call("timefield3d_set_yee_variant", grid.t,
+            {"flat": fd.YEE_FLAT, "flat4": fd.YEE_FLAT4, "fused": fd.YEE_FUSED}[variant])
     fused_problem(fd.lib, grid.t, dims, lossy)
     g = oracle_copy(orc, grid)
     if boundary == "cpml":
@@ -141,8 +143,12 @@ def test_fused_f32_matches_oracle(fd, orc, gpu, dims, boundary, lossy, variant):
         launches.append(fd.lib.fdtd_launch_count() - l0)
         g.step(dt)
     fd.check("fused loop")
-    # Yee kernels (2 flat, 1 fused) + the step counter
-    assert max(launches[5:]) == (3 if variant == "flat" else 2)
+    # Yee kernels + the step counter: 1 fused; 2 flat; flat4 2, or with a CPML
+    # 2 x 3 (interior box, z-slab planes, ring of the middle planes)
+    expect = {"fused": 2, "flat": 3, "flat4": 3}[variant]
+    if variant == "flat4" and nx % 4 == 0 and boundary == "cpml":
+        expect = 7
+    assert max(launches[5:]) == expect
     a, b = grid.fields(), g.fields()
     err = np.abs(a - b).max() / np.abs(b).max()
     assert np.abs(b).max() > 1e-3

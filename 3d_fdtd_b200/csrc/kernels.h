@@ -74,8 +74,9 @@ struct FlatArgs {
 void launch_flat_step(const FlatArgs &a, cudaStream_t st, cudaEvent_t mid);
 int flat4_supported(int nx, int nz);
 // cells of one flat4 launch: planes kA..kA+nA-1 then kB.., `count` (group, row)
-// slots per plane laid out by region kind (0 whole planes, 1 interior box
-// [gL, gR) x [L, ny-L), 2 the ring of y-slab rows and x-slab groups around it)
+// slots per plane laid out by region kind: 0 whole planes, 1 interior box
+// [gL, gR) x [L, ny-L), 3 y-slab rows x [gL, gR), 4 all rows x the columns
+// outside [gL, gR)
 struct Region4 {
     int kA, nA, kB;
     int count;

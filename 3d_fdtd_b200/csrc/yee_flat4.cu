@@ -17,14 +17,18 @@
 //
 // Regions.  Threads are laid out per z-plane over (group, row) slots.  A grid
 // without CPML runs whole planes k = 1..nz-2 with W = 4 (kind 0).  With a CPML
-// the slab instantiation holds far more state (auxiliaries, profiles), yet
-// inside the box [L, N-L) of every axis it computes exactly what the plain
-// instantiation computes (kappa = 1, auxiliaries 0).  So a CPML grid launches
-// the plain W = 4 kernel over that interior box (kind 1) and the CPML kernel
-// with W = 2, half the per-thread state and so twice the resident warps, over
-// the shell around it: the z-slab planes whole (kind 0) and, in the middle
-// planes, the ring of y-slab rows plus the x-slab groups of the other rows
-// (kind 2).  The shell runs on a second stream beside the box.
+// the slab code holds far more state (auxiliaries, profiles), yet inside the
+// box [L, N-L) of every axis it computes exactly what the plain code computes
+// (kappa = 1, auxiliaries 0).  So a CPML grid splits every update into four
+// launches, each compiled with only the slab terms its cells need (template
+// mask SLABS: 1 x, 2 y, 4 z):
+//   z-slab planes 1..L-1, nz-L..nz-2, whole        kind 0, SLABS 7, W 2
+//   middle planes, y-slab rows x box columns        kind 3, SLABS 2, W 4
+//   middle planes, all rows x x-slab columns        kind 4, SLABS 3, W 2
+//   middle planes, interior box                     kind 1, SLABS 0, W 4
+// W = 2 where the x-slab state (per element) would not fit two resident
+// blocks per SM at W = 4.  The shell launches run on a second stream beside
+// the box.
 //
 // CPML auxiliaries: the y- and z-slab ones are contiguous in x and move as
 // vectors; the x-slab ones (the groups at each end of a row) per element.
@@ -94,13 +98,13 @@ template <int W> struct XSlab {
 };
 
 // A0 = 0 for E (auxiliaries 0, 1; profiles 0..2), 2 for H (auxiliaries 2, 3; profiles 3..5)
-template <int W, int A0>
+template <int W, int A0, int SLABS>
 __device__ __forceinline__ void xslab_load(XSlab<W> &x, const FlatArgs &a, int g, int j, int k)
 {
     const int nx = a.nx, L = a.L;
     const int i0 = W * g;
     constexpr int pw = A0 == 0 ? 0 : 3;
-    x.any = i0 < L || i0 + W - 1 >= nx - L;
+    x.any = (SLABS & 1) && (i0 < L || i0 + W - 1 >= nx - L);
     x.s0 = 2LL * L * (j + (long long)a.ny * k);
 #pragma unroll
     for (int e = 0; e < W; e++) {
@@ -119,10 +123,10 @@ __device__ __forceinline__ void xslab_load(XSlab<W> &x, const FlatArgs &a, int g
     }
 }
 
-template <int W, int A0>
+template <int W, int A0, int SLABS>
 __device__ __forceinline__ void xslab_store(const XSlab<W> &x, const FlatArgs &a, int g)
 {
-    if (!x.any) return;
+    if (!(SLABS & 1) || !x.any) return;
 #pragma unroll
     for (int e = 0; e < W; e++) {
         if (!x.valid[e]) continue;
@@ -140,14 +144,14 @@ template <int W> struct YZSlab {
     long long sy, sz;
 };
 
-template <int W, int A0>
+template <int W, int A0, int SLABS>
 __device__ __forceinline__ void yzslab_load(YZSlab<W> &s, const FlatArgs &a, int g, int j, int k, long long ij0,
                                             long long nxy)
 {
     const int L = a.L;
     constexpr int pw = A0 == 0 ? 0 : 3;
-    s.sj = slab_local(j, a.ny, L);
-    s.sk = slab_local(k, a.nz, L);
+    s.sj = (SLABS & 2) ? slab_local(j, a.ny, L) : -1;
+    s.sk = (SLABS & 4) ? slab_local(k, a.nz, L) : -1;
     s.by = 1.f; s.ay = 0.f; s.ky = 1.f; s.bz = 1.f; s.az = 0.f; s.kz = 1.f;
     s.pxy = fillv<W>(0.f); s.pzy = s.pxy; s.pxz = s.pxy; s.pyz = s.pxy;
     s.sy = 0; s.sz = 0;
@@ -165,14 +169,14 @@ __device__ __forceinline__ void yzslab_load(YZSlab<W> &s, const FlatArgs &a, int
     }
 }
 
-template <int W, int A0>
+template <int W, int A0, int SLABS>
 __device__ __forceinline__ void yzslab_store(const YZSlab<W> &s, const FlatArgs &a)
 {
-    if (s.sj >= 0) {
+    if ((SLABS & 2) && s.sj >= 0) {
         stv<W>(a.psi[1][A0] + s.sy, s.pxy);
         stv<W>(a.psi[1][A0 + 1] + s.sy, s.pzy);
     }
-    if (s.sk >= 0) {
+    if ((SLABS & 4) && s.sk >= 0) {
         stv<W>(a.psi[2][A0] + s.sz, s.pxz);
         stv<W>(a.psi[2][A0 + 1] + s.sz, s.pyz);
     }
@@ -182,32 +186,32 @@ __device__ __forceinline__ void yzslab_store(const YZSlab<W> &s, const FlatArgs 
 // component (e.g. dHz/dy, dHy/dz for x); the auxiliaries update in place.
 struct Curl3 { float x, y, z; };
 
-template <int W>
+template <int W, int SLABS>
 __device__ __forceinline__ Curl3 cpml_curl(XSlab<W> &xs, YZSlab<W> &s, int e, float d_zy, float d_yz, float d_xz,
                                            float d_zx, float d_yx, float d_xy, float dx, float div)
 {
     // d_ab = difference of component a along axis b
     float pyx = 0.f, pzx = 0.f;
-    if (xs.valid[e]) {
+    if ((SLABS & 1) && xs.valid[e]) {
         pyx = xs.b[e] * xs.p0[e] + xs.c[e] * (d_zx * div);
         pzx = xs.b[e] * xs.p1[e] + xs.c[e] * (d_yx * div);
         xs.p0[e] = pyx;
         xs.p1[e] = pzx;
     }
     float vxy = 0.f, vzy = 0.f, vxz = 0.f, vyz = 0.f;
-    if (s.sj >= 0) {
+    if ((SLABS & 2) && s.sj >= 0) {
         vxy = s.by * s.pxy.v[e] + s.ay * (d_zy * div);
         vzy = s.by * s.pzy.v[e] + s.ay * (d_xy * div);
         s.pxy.v[e] = vxy;
         s.pzy.v[e] = vzy;
     }
-    if (s.sk >= 0) {
+    if ((SLABS & 4) && s.sk >= 0) {
         vxz = s.bz * s.pxz.v[e] + s.az * (d_yz * div);
         vyz = s.bz * s.pyz.v[e] + s.az * (d_xz * div);
         s.pxz.v[e] = vxz;
         s.pyz.v[e] = vyz;
     }
-    const float kx = xs.k[e];
+    const float kx = (SLABS & 1) ? xs.k[e] : 1.f;
     Curl3 c;
     c.x = s.ky * d_zy - s.kz * d_yz + dx * (vxy - vxz);
     c.y = s.kz * d_xz - kx * d_zx + dx * (vyz - pyx);
@@ -215,7 +219,7 @@ __device__ __forceinline__ Curl3 cpml_curl(XSlab<W> &xs, YZSlab<W> &s, int e, fl
     return c;
 }
 
-// slot -> (group, row) of one region, and the plane of blockIdx.y
+// slot -> (group, row) of one region kind, and the plane of blockIdx.y
 template <int KIND>
 __device__ __forceinline__ void locate(const Region4 &r, int ngroups, int ny, int &g, int &j, int &k, bool &live)
 {
@@ -231,28 +235,26 @@ __device__ __forceinline__ void locate(const Region4 &r, int ngroups, int ny, in
         const int gw = r.gR - r.gL;
         g = r.gL + s % gw;
         j = r.L + s / gw;
+    } else if (KIND == 3) {
+        // rows 1..L-1 then ny-L..ny-2, columns [gL, gR)
+        const int gw = r.gR - r.gL;
+        const int row = s / gw;
+        g = r.gL + (s - row * gw);
+        j = row < r.L - 1 ? 1 + row : ny - r.L + (row - (r.L - 1));
     } else {
-        const int band = (r.L - 1) * ngroups;
-        if (s < band) {
-            g = s % ngroups;
-            j = 1 + s / ngroups;
-        } else if (s < 2 * band) {
-            s -= band;
-            g = s % ngroups;
-            j = ny - r.L + s / ngroups;
-        } else {
-            s -= 2 * band;
-            const int w = r.gL + ngroups - r.gR;
-            const int rr = s % w;
-            j = r.L + s / w;
-            g = rr < r.gL ? rr : r.gR + (rr - r.gL);
-        }
+        // rows 1..ny-2, columns [0, gL) then [gR, ngroups)
+        const int w = r.gL + ngroups - r.gR;
+        const int row = s / w;
+        const int rr = s - row * w;
+        j = 1 + row;
+        g = rr < r.gL ? rr : r.gR + (rr - r.gL);
     }
 }
 
-template <int W, bool CPML, bool LOSSY, int KIND>
-__global__ void __launch_bounds__(kBlock4, W == 4 ? 2 : 3) k_flat4_E(FlatArgs a, Region4 r)
+template <int W, int SLABS, bool LOSSY, int KIND>
+__global__ void __launch_bounds__(kBlock4, W == 4 ? (SLABS ? 2 : (LOSSY ? 3 : 4)) : 3) k_flat4_E(FlatArgs a, Region4 r)
 {
+    constexpr bool CPML = SLABS != 0;
     const int nx = a.nx, ny = a.ny;
     const int ngroups = nx / W;
     const int lane = threadIdx.x & 31;
@@ -290,18 +292,13 @@ __global__ void __launch_bounds__(kBlock4, W == 4 ? 2 : 3) k_flat4_E(FlatArgs a,
         c1 = ldv<W>(a.ca[1] + q0);
         c2 = ldv<W>(a.ca[2] + q0);
     }
+    // source planes are a few of the nz planes: their values load in phase 2
     const float *sp = a.src.n ? src_plane(a.src, k) : nullptr;
-    Vf<W> j0 = fillv<W>(0.f), j1 = j0, j2 = j0;
-    if (sp) {
-        j0 = ldv<W>(sp + ij0);
-        j1 = ldv<W>(sp + nxy + ij0);
-        j2 = ldv<W>(sp + 2 * nxy + ij0);
-    }
     XSlab<W> xs;
     YZSlab<W> ys;
     if (CPML) {
-        yzslab_load<W, 0>(ys, a, g, j, k, ij0, nxy);
-        xslab_load<W, 0>(xs, a, g, j, k);
+        yzslab_load<W, 0, SLABS>(ys, a, g, j, k, ij0, nxy);
+        xslab_load<W, 0, SLABS>(xs, a, g, j, k);
     }
     // ---- phase 2: arithmetic
     const float dx = a.dx, div = 1.0f / dx;
@@ -323,13 +320,13 @@ __global__ void __launch_bounds__(kBlock4, W == 4 ? 2 : 3) k_flat4_E(FlatArgs a,
             cy = dHx_dz - dHz_dx;
             cz = dHy_dx - dHx_dy;
         } else {
-            const Curl3 c = cpml_curl<W>(xs, ys, e, dHz_dy, dHy_dz, dHx_dz, dHz_dx, dHy_dx, dHx_dy, dx, div);
+            const Curl3 c = cpml_curl<W, SLABS>(xs, ys, e, dHz_dy, dHy_dz, dHx_dz, dHz_dx, dHy_dx, dHx_dy, dx, div);
             cx = c.x; cy = c.y; cz = c.z;
         }
         if (sp) {
-            cx -= dx * j0.v[e];
-            cy -= dx * j1.v[e];
-            cz -= dx * j2.v[e];
+            cx -= dx * __ldg(sp + ij0 + e);
+            cy -= dx * __ldg(sp + nxy + ij0 + e);
+            cz -= dx * __ldg(sp + 2 * nxy + ij0 + e);
         }
         ex.v[e] = c0.v[e] * ex.v[e] + b0.v[e] * cx;
         ey.v[e] = c1.v[e] * ey.v[e] + b1.v[e] * cy;
@@ -340,14 +337,15 @@ __global__ void __launch_bounds__(kBlock4, W == 4 ? 2 : 3) k_flat4_E(FlatArgs a,
     stv<W>(a.f[1] + q0, ey);
     stv<W>(a.f[2] + q0, ez);
     if (CPML) {
-        yzslab_store<W, 0>(ys, a);
-        xslab_store<W, 0>(xs, a, g);
+        yzslab_store<W, 0, SLABS>(ys, a);
+        xslab_store<W, 0, SLABS>(xs, a, g);
     }
 }
 
-template <int W, bool CPML, int KIND>
-__global__ void __launch_bounds__(kBlock4, W == 4 ? 2 : 3) k_flat4_H(FlatArgs a, Region4 r)
+template <int W, int SLABS, int KIND>
+__global__ void __launch_bounds__(kBlock4, W == 4 ? (SLABS ? 2 : 4) : 3) k_flat4_H(FlatArgs a, Region4 r)
 {
+    constexpr bool CPML = SLABS != 0;
     const int nx = a.nx, ny = a.ny;
     const int ngroups = nx / W;
     const int lane = threadIdx.x & 31;
@@ -378,17 +376,11 @@ __global__ void __launch_bounds__(kBlock4, W == 4 ? 2 : 3) k_flat4_H(FlatArgs a,
     const Vf<W> ex_kp = ldv<W>(a.f[0] + q0 + nxy), ey_kp = ldv<W>(a.f[1] + q0 + nxy);
     Vf<W> hx = ldv_rw<W>(a.f[3] + q0), hy = ldv_rw<W>(a.f[4] + q0), hz = ldv_rw<W>(a.f[5] + q0);
     const float *sp = a.src.n ? src_plane(a.src, k) : nullptr;
-    Vf<W> m0 = fillv<W>(0.f), m1 = m0, m2 = m0;
-    if (sp) {
-        m0 = ldv<W>(sp + 3 * nxy + ij0);
-        m1 = ldv<W>(sp + 4 * nxy + ij0);
-        m2 = ldv<W>(sp + 5 * nxy + ij0);
-    }
     XSlab<W> xs;
     YZSlab<W> ys;
     if (CPML) {
-        yzslab_load<W, 2>(ys, a, g, j, k, ij0, nxy);
-        xslab_load<W, 2>(xs, a, g, j, k);
+        yzslab_load<W, 2, SLABS>(ys, a, g, j, k, ij0, nxy);
+        xslab_load<W, 2, SLABS>(xs, a, g, j, k);
     }
     // ---- phase 2: arithmetic
     const float dx = a.dx, hb = a.hb, div = 1.0f / dx;
@@ -410,13 +402,13 @@ __global__ void __launch_bounds__(kBlock4, W == 4 ? 2 : 3) k_flat4_H(FlatArgs a,
             cy = dEx_dz - dEz_dx;
             cz = dEy_dx - dEx_dy;
         } else {
-            const Curl3 c = cpml_curl<W>(xs, ys, e, dEz_dy, dEy_dz, dEx_dz, dEz_dx, dEy_dx, dEx_dy, dx, div);
+            const Curl3 c = cpml_curl<W, SLABS>(xs, ys, e, dEz_dy, dEy_dz, dEx_dz, dEz_dx, dEy_dx, dEx_dy, dx, div);
             cx = c.x; cy = c.y; cz = c.z;
         }
         if (sp) {
-            cx += dx * m0.v[e];
-            cy += dx * m1.v[e];
-            cz += dx * m2.v[e];
+            cx += dx * __ldg(sp + 3 * nxy + ij0 + e);
+            cy += dx * __ldg(sp + 4 * nxy + ij0 + e);
+            cz += dx * __ldg(sp + 5 * nxy + ij0 + e);
         }
         hx.v[e] = hx.v[e] - hb * cx;
         hy.v[e] = hy.v[e] - hb * cy;
@@ -427,8 +419,8 @@ __global__ void __launch_bounds__(kBlock4, W == 4 ? 2 : 3) k_flat4_H(FlatArgs a,
     stv<W>(a.f[4] + q0, hy);
     stv<W>(a.f[5] + q0, hz);
     if (CPML) {
-        yzslab_store<W, 2>(ys, a);
-        xslab_store<W, 2>(xs, a, g);
+        yzslab_store<W, 2, SLABS>(ys, a);
+        xslab_store<W, 2, SLABS>(xs, a, g);
     }
 }
 
@@ -441,23 +433,32 @@ static Region4 planes_region(int kA, int nA, int kB, int count)
     return r;
 }
 
-// kernel instantiations per launch: kind 1 -> plain W=4 box; kind 2 -> CPML W=2 ring;
-// kind 0 -> CPML W=2 z-slab planes, or plain W=4 whole planes of a grid without CPML
+// kernel instantiation per launch kind; kind 0 is the CPML z-slab planes (or
+// whole planes of a CPML grid that does not split) when `cpml`, else the whole
+// planes of a grid without CPML
 template <bool LOSSY>
 static void launch_E(const FlatArgs &a, const Region4 &r, dim3 grid, int kind, bool cpml, cudaStream_t st)
 {
-    if (kind == 1) k_flat4_E<4, false, LOSSY, 1><<<grid, kBlock4, 0, st>>>(a, r);
-    else if (kind == 2) k_flat4_E<2, true, LOSSY, 2><<<grid, kBlock4, 0, st>>>(a, r);
-    else if (cpml) k_flat4_E<2, true, LOSSY, 0><<<grid, kBlock4, 0, st>>>(a, r);
-    else k_flat4_E<4, false, LOSSY, 0><<<grid, kBlock4, 0, st>>>(a, r);
+    switch (kind) {
+    case 1: k_flat4_E<4, 0, LOSSY, 1><<<grid, kBlock4, 0, st>>>(a, r); break;
+    case 3: k_flat4_E<4, 2, LOSSY, 3><<<grid, kBlock4, 0, st>>>(a, r); break;
+    case 4: k_flat4_E<2, 3, LOSSY, 4><<<grid, kBlock4, 0, st>>>(a, r); break;
+    default:
+        if (cpml) k_flat4_E<2, 7, LOSSY, 0><<<grid, kBlock4, 0, st>>>(a, r);
+        else k_flat4_E<4, 0, LOSSY, 0><<<grid, kBlock4, 0, st>>>(a, r);
+    }
 }
 
 static void launch_H(const FlatArgs &a, const Region4 &r, dim3 grid, int kind, bool cpml, cudaStream_t st)
 {
-    if (kind == 1) k_flat4_H<4, false, 1><<<grid, kBlock4, 0, st>>>(a, r);
-    else if (kind == 2) k_flat4_H<2, true, 2><<<grid, kBlock4, 0, st>>>(a, r);
-    else if (cpml) k_flat4_H<2, true, 0><<<grid, kBlock4, 0, st>>>(a, r);
-    else k_flat4_H<4, false, 0><<<grid, kBlock4, 0, st>>>(a, r);
+    switch (kind) {
+    case 1: k_flat4_H<4, 0, 1><<<grid, kBlock4, 0, st>>>(a, r); break;
+    case 3: k_flat4_H<4, 2, 3><<<grid, kBlock4, 0, st>>>(a, r); break;
+    case 4: k_flat4_H<2, 3, 4><<<grid, kBlock4, 0, st>>>(a, r); break;
+    default:
+        if (cpml) k_flat4_H<2, 7, 0><<<grid, kBlock4, 0, st>>>(a, r);
+        else k_flat4_H<4, 0, 0><<<grid, kBlock4, 0, st>>>(a, r);
+    }
 }
 
 static void launch_phase(bool e_phase, const FlatArgs &a, const Region4 &r, int nplanes, int kind, bool cpml,
@@ -490,30 +491,31 @@ void launch_flat4_step(const FlatArgs &a, cudaStream_t st, cudaStream_t side, cu
         return;
     }
     if (!side || !flat4_split_supported(a)) {
-        // CPML kernel (W = 2) over whole planes
+        // CPML code (W = 2) over whole planes
         const Region4 r = planes_region(1, nz - 2, 0, (nx / 2) * ny);
         launch_phase(true, a, r, nz - 2, 0, true, st);
         launch_phase(false, a, r, nz - 2, 0, true, st);
         return;
     }
-    const int L = a.L, ng2 = nx / 2;
-    // interior box in 4-cell groups [gL, gR): every cell of it lies in [L, nx-L)
+    const int L = a.L, ng2 = nx / 2, nmid = nz - 2 * L;
+    // box columns in 4-cell groups [gL, gR): every cell of them lies in [L, nx-L)
     const int gL = (L + 3) / 4, gR = (nx - L) / 4;
-    Region4 box = planes_region(L, nz - 2 * L, 0, (gR - gL) * (ny - 2 * L));
+    Region4 box = planes_region(L, nmid, 0, (gR - gL) * (ny - 2 * L));
     box.gL = gL; box.gR = gR; box.L = L;
-    // shell in 2-cell groups: z-slab planes 1..L-1 and nz-L..nz-2 whole, and in
-    // the middle planes the ring around the box (its groups [2 gL, 2 gR) excluded)
+    Region4 yrows = planes_region(L, nmid, 0, 2 * (L - 1) * (gR - gL));
+    yrows.gL = gL; yrows.gR = gR; yrows.L = L;
+    // x-slab columns in 2-cell groups: [0, 2 gL) and [2 gR, ng2)
+    Region4 xcols = planes_region(L, nmid, 0, (ny - 2) * (2 * gL + ng2 - 2 * gR));
+    xcols.gL = 2 * gL; xcols.gR = 2 * gR; xcols.L = L;
     const Region4 zs = planes_region(1, L - 1, nz - L, ng2 * ny);
-    Region4 ring = planes_region(L, nz - 2 * L, 0,
-                                 2 * (L - 1) * ng2 + (ny - 2 * L) * (2 * gL + ng2 - 2 * gR));
-    ring.gL = 2 * gL; ring.gR = 2 * gR; ring.L = L;
     for (int phase = 0; phase < 2; phase++) {
         const bool e = phase == 0;
         cudaEventRecord(fork, st);
         cudaStreamWaitEvent(side, fork, 0);
         launch_phase(e, a, zs, 2 * (L - 1), 0, true, side);
-        launch_phase(e, a, ring, nz - 2 * L, 2, true, side);
-        launch_phase(e, a, box, nz - 2 * L, 1, false, st);
+        launch_phase(e, a, xcols, nmid, 4, true, side);
+        launch_phase(e, a, yrows, nmid, 3, true, side);
+        launch_phase(e, a, box, nmid, 1, false, st);
         cudaEventRecord(join, side);
         cudaStreamWaitEvent(st, join, 0);
     }

@@ -82,6 +82,13 @@ struct Region4 {
     int count;
     int gL, gR, L;
 };
+// block plan of the merged CPML launch: z-slab planes get nbz blocks each,
+// middle planes nbm = nb_box + nb_y + nb_x
+struct Plan4 {
+    int L, nmid;
+    int nbz, nbm, nb_box, nb_y;
+    Region4 zs, box, yrows, xcols;
+};
 bool flat4_split_supported(const FlatArgs &a);
 // E then H update.  With a CPML and a side stream the interior box runs on `st`
 // and the shell on `side` (fork/join through the two events) for each field.

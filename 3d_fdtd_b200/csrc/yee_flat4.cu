@@ -221,10 +221,9 @@ __device__ __forceinline__ Curl3 cpml_curl(XSlab<W> &xs, YZSlab<W> &s, int e, fl
 
 // slot -> (group, row) of one region kind, and the plane of blockIdx.y
 template <int KIND>
-__device__ __forceinline__ void locate(const Region4 &r, int ngroups, int ny, int &g, int &j, int &k, bool &live)
+__device__ __forceinline__ void locate(const Region4 &r, int ngroups, int ny, int s, int by, int &g, int &j, int &k,
+                                       bool &live)
 {
-    int s = blockIdx.x * kBlock4 + threadIdx.x;
-    const int by = blockIdx.y;
     k = by < r.nA ? r.kA + by : r.kB + (by - r.nA);
     live = s < r.count;
     if (KIND == 0) {
@@ -251,16 +250,14 @@ __device__ __forceinline__ void locate(const Region4 &r, int ngroups, int ny, in
     }
 }
 
-template <int W, int SLABS, bool LOSSY, int KIND>
-__global__ void __launch_bounds__(kBlock4, W == 4 ? (SLABS ? 2 : (LOSSY ? 3 : 4)) : 3) k_flat4_E(FlatArgs a, Region4 r)
+// E update of the W cells of group g, row j, plane k (all lanes of the warp call it)
+template <int W, int SLABS, bool LOSSY>
+__device__ __forceinline__ void e_cells(const FlatArgs &a, int g, int j, int k, bool live)
 {
     constexpr bool CPML = SLABS != 0;
     const int nx = a.nx, ny = a.ny;
     const int ngroups = nx / W;
     const int lane = threadIdx.x & 31;
-    int g, j, k;
-    bool live;
-    locate<KIND>(r, ngroups, ny, g, j, k, live);
     const long long nxy = (long long)nx * ny;
     const long long ij0 = (long long)W * g + (long long)nx * j;
     const long long q0 = ij0 + nxy * k;
@@ -342,16 +339,14 @@ __global__ void __launch_bounds__(kBlock4, W == 4 ? (SLABS ? 2 : (LOSSY ? 3 : 4)
     }
 }
 
-template <int W, int SLABS, int KIND>
-__global__ void __launch_bounds__(kBlock4, W == 4 ? (SLABS ? 2 : 4) : 3) k_flat4_H(FlatArgs a, Region4 r)
+// H update of the W cells of group g, row j, plane k (all lanes of the warp call it)
+template <int W, int SLABS>
+__device__ __forceinline__ void h_cells(const FlatArgs &a, int g, int j, int k, bool live)
 {
     constexpr bool CPML = SLABS != 0;
     const int nx = a.nx, ny = a.ny;
     const int ngroups = nx / W;
     const int lane = threadIdx.x & 31;
-    int g, j, k;
-    bool live;
-    locate<KIND>(r, ngroups, ny, g, j, k, live);
     const long long nxy = (long long)nx * ny;
     const long long ij0 = (long long)W * g + (long long)nx * j;
     const long long q0 = ij0 + nxy * k;
@@ -421,6 +416,74 @@ __global__ void __launch_bounds__(kBlock4, W == 4 ? (SLABS ? 2 : 4) : 3) k_flat4
     if (CPML) {
         yzslab_store<W, 2, SLABS>(ys, a);
         xslab_store<W, 2, SLABS>(xs, a, g);
+    }
+}
+
+template <int W, int SLABS, bool LOSSY, int KIND>
+__global__ void __launch_bounds__(kBlock4, W == 4 ? (SLABS ? 2 : (LOSSY ? 3 : 4)) : 3) k_flat4_E(FlatArgs a, Region4 r)
+{
+    int g, j, k;
+    bool live;
+    locate<KIND>(r, a.nx / W, a.ny, blockIdx.x * kBlock4 + threadIdx.x, blockIdx.y, g, j, k, live);
+    e_cells<W, SLABS, LOSSY>(a, g, j, k, live);
+}
+
+template <int W, int SLABS, int KIND>
+__global__ void __launch_bounds__(kBlock4, W == 4 ? (SLABS ? 2 : 4) : 3) k_flat4_H(FlatArgs a, Region4 r)
+{
+    int g, j, k;
+    bool live;
+    locate<KIND>(r, a.nx / W, a.ny, blockIdx.x * kBlock4 + threadIdx.x, blockIdx.y, g, j, k, live);
+    h_cells<W, SLABS>(a, g, j, k, live);
+}
+
+// One launch per field over a CPML grid: blocks in plane order, each plane's
+// blocks split between the regions present in it (block-uniform branch).
+//   planes 1..L-1, nz-L..nz-2: nbz blocks of the z-slab region (W 2, SLABS 7)
+//   planes L..nz-L-1: nb_box box blocks (W 4, plain), nb_y y-slab-row blocks
+//   (W 2, SLABS 2), nb_x x-slab-column blocks (W 2, SLABS 3)
+template <bool E_FIELD, bool LOSSY>
+__global__ void __launch_bounds__(kBlock4, 3) k_flat4_merged(FlatArgs a, Plan4 p)
+{
+    int b = blockIdx.x;
+    const int nzs = (p.L - 1) * p.nbz, nmb = p.nmid * p.nbm;
+    int plane, lb;
+    bool zslab;
+    if (b < nzs) {
+        zslab = true;
+        plane = b / p.nbz;
+        lb = b - plane * p.nbz;
+    } else if (b < nzs + nmb) {
+        zslab = false;
+        b -= nzs;
+        plane = b / p.nbm;
+        lb = b - plane * p.nbm;
+    } else {
+        zslab = true;
+        b -= nzs + nmb;
+        const int q = b / p.nbz;
+        lb = b - q * p.nbz;
+        plane = (p.L - 1) + q;  // index into zs (its second plane range)
+    }
+    const int t = threadIdx.x;
+    int g, j, k;
+    bool live;
+    if (zslab) {
+        locate<0>(p.zs, a.nx / 2, a.ny, lb * kBlock4 + t, plane, g, j, k, live);
+        if (E_FIELD) e_cells<2, 7, LOSSY>(a, g, j, k, live);
+        else h_cells<2, 7>(a, g, j, k, live);
+    } else if (lb < p.nb_box) {
+        locate<1>(p.box, a.nx / 4, a.ny, lb * kBlock4 + t, plane, g, j, k, live);
+        if (E_FIELD) e_cells<4, 0, LOSSY>(a, g, j, k, live);
+        else h_cells<4, 0>(a, g, j, k, live);
+    } else if (lb < p.nb_box + p.nb_y) {
+        locate<3>(p.yrows, a.nx / 2, a.ny, (lb - p.nb_box) * kBlock4 + t, plane, g, j, k, live);
+        if (E_FIELD) e_cells<2, 2, LOSSY>(a, g, j, k, live);
+        else h_cells<2, 2>(a, g, j, k, live);
+    } else {
+        locate<4>(p.xcols, a.nx / 2, a.ny, (lb - p.nb_box - p.nb_y) * kBlock4 + t, plane, g, j, k, live);
+        if (E_FIELD) e_cells<2, 3, LOSSY>(a, g, j, k, live);
+        else h_cells<2, 3>(a, g, j, k, live);
     }
 }
 
@@ -498,27 +561,34 @@ void launch_flat4_step(const FlatArgs &a, cudaStream_t st, cudaStream_t side, cu
         return;
     }
     const int L = a.L, ng2 = nx / 2, nmid = nz - 2 * L;
-    // box columns in 4-cell groups [gL, gR): every cell of them lies in [L, nx-L)
-    const int gL = (L + 3) / 4, gR = (nx - L) / 4;
-    Region4 box = planes_region(L, nmid, 0, (gR - gL) * (ny - 2 * L));
-    box.gL = gL; box.gR = gR; box.L = L;
-    Region4 yrows = planes_region(L, nmid, 0, 2 * (L - 1) * (gR - gL));
-    yrows.gL = gL; yrows.gR = gR; yrows.L = L;
-    // x-slab columns in 2-cell groups: [0, 2 gL) and [2 gR, ng2)
-    Region4 xcols = planes_region(L, nmid, 0, (ny - 2) * (2 * gL + ng2 - 2 * gR));
-    xcols.gL = 2 * gL; xcols.gR = 2 * gR; xcols.L = L;
-    const Region4 zs = planes_region(1, L - 1, nz - L, ng2 * ny);
-    for (int phase = 0; phase < 2; phase++) {
-        const bool e = phase == 0;
-        cudaEventRecord(fork, st);
-        cudaStreamWaitEvent(side, fork, 0);
-        launch_phase(e, a, zs, 2 * (L - 1), 0, true, side);
-        launch_phase(e, a, xcols, nmid, 4, true, side);
-        launch_phase(e, a, yrows, nmid, 3, true, side);
-        launch_phase(e, a, box, nmid, 1, false, st);
-        cudaEventRecord(join, side);
-        cudaStreamWaitEvent(st, join, 0);
+    const int gL = (L + 3) / 4, gR = (nx - L) / 4;  // box columns in 4-cell groups
+    Plan4 p{};
+    p.L = L;
+    p.nmid = nmid;
+    p.zs = planes_region(1, L - 1, nz - L, ng2 * ny);
+    p.box = planes_region(L, nmid, 0, (gR - gL) * (ny - 2 * L));
+    p.box.gL = gL; p.box.gR = gR; p.box.L = L;
+    // shell columns in 2-cell groups: [2 gL, 2 gR) for the y-slab rows, the rest for the x-slab columns
+    p.yrows = planes_region(L, nmid, 0, 2 * (L - 1) * (2 * gR - 2 * gL));
+    p.yrows.gL = 2 * gL; p.yrows.gR = 2 * gR; p.yrows.L = L;
+    p.xcols = planes_region(L, nmid, 0, (ny - 2) * (2 * gL + ng2 - 2 * gR));
+    p.xcols.gL = 2 * gL; p.xcols.gR = 2 * gR; p.xcols.L = L;
+    auto nblk = [](int count) { return (count + kBlock4 - 1) / kBlock4; };
+    p.nbz = nblk(p.zs.count);
+    p.nb_box = nblk(p.box.count);
+    p.nb_y = nblk(p.yrows.count);
+    p.nbm = p.nb_box + p.nb_y + nblk(p.xcols.count);
+    const long long blocks = 2LL * (L - 1) * p.nbz + (long long)nmid * p.nbm;
+    const bool lossy = a.ca[0] != nullptr;
+    note_launch(2);
+    if (lossy) {
+        k_flat4_merged<true, true><<<(unsigned)blocks, kBlock4, 0, st>>>(a, p);
+        k_flat4_merged<false, true><<<(unsigned)blocks, kBlock4, 0, st>>>(a, p);
+    } else {
+        k_flat4_merged<true, false><<<(unsigned)blocks, kBlock4, 0, st>>>(a, p);
+        k_flat4_merged<false, false><<<(unsigned)blocks, kBlock4, 0, st>>>(a, p);
     }
+    (void)side; (void)fork; (void)join;
 }
 
 }  // namespace fdtd

@@ -21,39 +21,37 @@ namespace fdtd {
 // reference, and passed in; sched != null selects per-step values indexed by
 // the device step counter.
 // ---------------------------------------------------------------------------
-__global__ void k_mode_source(float *plane, const float *ep_plane0, const float *ep_plane1, const float *ep_plane2,
-                              const float *mu_plane0, const float *mu_plane1, const float *mu_plane2, int nx,
-                              int ny, int cx, int cy, const double2 *mode, int mi, int mj, double ratio,
-                              double amplitude, double cph, double sph, const double *sched,
-                              const long long *step, int nsched, int reverse, int adjoint)
+__device__ __forceinline__ void schedule_values(const SourceJob &sj, long long n, double &A, double &c, double &s)
 {
-    const long long nxy = (long long)nx * ny;
-    double A = amplitude, c = cph, s = sph;
-    if (sched) {
-        long long n = *step;
-        if (n < 0 || n >= nsched) {
-            A = 0.0; c = 0.0; s = 0.0;   // outside the schedule: zero source
-        } else {
-            A = sched[3 * n]; c = sched[3 * n + 1]; s = sched[3 * n + 2];
-        }
+    if (n < 0 || n >= sj.nsched) {
+        A = 0.0; c = 0.0; s = 0.0;   // outside the schedule: zero source
+    } else {
+        A = sj.sched[3 * n]; c = sj.sched[3 * n + 1]; s = sj.sched[3 * n + 2];
     }
-    const int M_sign = -1 + 2 * reverse;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nxy; t += (long long)gridDim.x * blockDim.x) {
+}
+
+// cells t = first, first + stride, ... of the source plane
+__device__ __forceinline__ void mode_source_cells(const SourceJob &sj, long long first, long long stride, double A,
+                                                  double c, double s)
+{
+    const int nx = sj.nx;
+    const long long nxy = (long long)nx * sj.ny;
+    const int M_sign = -1 + 2 * sj.reverse;
+    float *plane = sj.plane;
+    for (long long t = first; t < nxy; t += stride) {
         int i = (int)(t % nx), j = (int)(t / nx);
-        double xd = dmul((double)(i - cx), ratio);
-        double yd = dmul((double)(j - cy), ratio);
-        int mx = (int)xd + mi / 2, my = (int)yd + mj / 2;
-        if (mx < 0 || mx >= mi || my < 0 || my >= mj) continue;
-        const double2 *e = mode + 6LL * (mx + (long long)mi * my);
-        if (!adjoint) {
-            const float *epp[3] = {ep_plane0, ep_plane1, ep_plane2};
-            const float *mup[3] = {mu_plane0, mu_plane1, mu_plane2};
+        double xd = dmul((double)(i - sj.cx), sj.ratio);
+        double yd = dmul((double)(j - sj.cy), sj.ratio);
+        int mx = (int)xd + sj.mi / 2, my = (int)yd + sj.mj / 2;
+        if (mx < 0 || mx >= sj.mi || my < 0 || my >= sj.mj) continue;
+        const double2 *e = sj.mode + 6LL * (mx + (long long)sj.mi * my);
+        if (!sj.adjoint) {
 #pragma unroll
             for (int m = 0; m < 6; m++) {
                 double proj = dadd(dmul(e[m].x, c), dmul(e[m].y, s));
                 double v;
-                if (m < 3) v = dmul(dmul(A, (double)epp[m][t]), proj);
-                else v = dmul(dmul(dmul((double)(-M_sign), A), (double)mup[m - 3][t]), proj);
+                if (m < 3) v = dmul(dmul(A, (double)sj.ep[m][t]), proj);
+                else v = dmul(dmul(dmul((double)(-M_sign), A), (double)sj.mu[m - 3][t]), proj);
                 plane[m * nxy + t] = __double2float_rn(v);
             }
         } else {
@@ -67,6 +65,15 @@ __global__ void k_mode_source(float *plane, const float *ep_plane0, const float 
     }
 }
 
+// fixed amplitude and phase, or (sched != null) the schedule entry of step *step + offset
+__global__ void k_mode_source(SourceJob sj, double amplitude, double cph, double sph, const long long *step,
+                              int step_offset)
+{
+    double A = amplitude, c = cph, s = sph;
+    if (sj.sched) schedule_values(sj, *step + step_offset, A, c, s);
+    mode_source_cells(sj, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x, A, c, s);
+}
+
 __global__ void k_set_value(float *p, long long idx, float v) { p[idx] = v; }
 
 // ---------------------------------------------------------------------------
@@ -78,16 +85,17 @@ __global__ void k_set_value(float *p, long long idx, float v) { p[idx] = v; }
 // monitors, accumulates e^{i omega n dt} o(n) per frequency with Kahan
 // compensation.
 // ---------------------------------------------------------------------------
+// partial `part` of `nparts` of one job's plane sum, written to *out (all
+// threads of the block call it)
 template <typename T>
-__global__ void k_overlap_partial(const T *const *Ex_, int nx, int ny, const OverlapJob *jobs, double2 *partials,
-                                  int nparts)
+__device__ __forceinline__ void overlap_block(const T *const *Ex_, int nx, int ny, const OverlapJob &jb, int part,
+                                              int nparts, double2 *out)
 {
-    const OverlapJob jb = jobs[blockIdx.y];
     const long long nxy = (long long)nx * ny;
     const T *Ex = Ex_[0], *Ey = Ex_[1], *Hx = Ex_[3], *Hy = Ex_[4];
     const long long base = nxy * jb.cz;
     double sre = 0.0, sim = 0.0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nxy; t += (long long)gridDim.x * blockDim.x) {
+    for (long long t = part * (long long)blockDim.x + threadIdx.x; t < nxy; t += (long long)nparts * blockDim.x) {
         int i = (int)(t % nx), j = (int)(t / nx);
         double xd = dmul((double)(i - jb.cx), jb.ratio);
         double yd = dmul((double)(j - jb.cy), jb.ratio);
@@ -122,8 +130,16 @@ __global__ void k_overlap_partial(const T *const *Ex_, int nx, int ny, const Ove
             v.x = dadd(v.x, __shfl_down_sync(0xffffffffu, v.x, o));
             v.y = dadd(v.y, __shfl_down_sync(0xffffffffu, v.y, o));
         }
-        if (lane == 0) partials[(long long)blockIdx.y * nparts + blockIdx.x] = v;
+        if (lane == 0) *out = v;
     }
+}
+
+template <typename T>
+__global__ void k_overlap_partial(const T *const *Ex_, int nx, int ny, const OverlapJob *jobs, double2 *partials,
+                                  int nparts)
+{
+    const OverlapJob jb = jobs[blockIdx.y];
+    overlap_block<T>(Ex_, nx, ny, jb, blockIdx.x, nparts, partials + (long long)blockIdx.y * nparts + blockIdx.x);
 }
 
 // reduce_phase: phase - (int)(phase/(2 pi)) 2 pi with the reference's 9-digit pi
@@ -135,17 +151,33 @@ __device__ __forceinline__ double reduce_phase(double ph)
     return dsub(ph, dmul(q, two_pi));
 }
 
-__global__ void k_overlap_finalize(const OverlapJob *jobs, int njobs, const double2 *partials, int nparts,
-                                   double scale, double dt, const long long *step, int step_offset)
+// acc[2f] += e^{i omega_f n dt} o with Kahan compensation in acc[2f+1]
+__device__ __forceinline__ void accumulate_frequency(const OverlapJob &jb, int f, double2 o, double dt, long long n)
 {
-    const int jid = blockIdx.x;
-    if (jid >= njobs) return;
-    const OverlapJob jb = jobs[jid];
+    double ph = reduce_phase(dmul(dmul((double)n, dt), jb.omega[f]));
+    double s, c;
+    sincos(ph, &s, &c);
+    double add_re = dsub(dmul(c, o.x), dmul(s, o.y));
+    double add_im = dadd(dmul(c, o.y), dmul(s, o.x));
+    double2 sum = jb.acc[2 * f], comp = jb.acc[2 * f + 1];
+    double yr = dsub(add_re, comp.x), yi = dsub(add_im, comp.y);
+    double tr = dadd(sum.x, yr), ti = dadd(sum.y, yi);
+    comp.x = dsub(dsub(tr, sum.x), yr);
+    comp.y = dsub(dsub(ti, sum.y), yi);
+    jb.acc[2 * f] = make_double2(tr, ti);
+    jb.acc[2 * f + 1] = comp;
+}
+
+// sum one job's partials in order, scale, store the instantaneous value and
+// accumulate e^{i omega n dt} o per frequency (all threads of the block call it)
+__device__ __forceinline__ void overlap_finalize_job(const OverlapJob &jb, const double2 *partials, int nparts,
+                                                     double scale, double dt, long long n)
+{
     __shared__ double2 tot;
     if (threadIdx.x == 0) {
         double sre = 0.0, sim = 0.0;
         for (int p = 0; p < nparts; p++) {
-            double2 v = partials[(long long)jid * nparts + p];
+            double2 v = partials[p];
             sre = dadd(sre, v.x);
             sim = dadd(sim, v.y);
         }
@@ -154,31 +186,98 @@ __global__ void k_overlap_finalize(const OverlapJob *jobs, int njobs, const doub
     }
     __syncthreads();
     if (!jb.acc) return;
-    const long long n = *step + step_offset;
     const double2 o = tot;
-    // one thread per frequency: acc[2f] = sum, acc[2f+1] = Kahan compensation
-    for (int f = threadIdx.x; f < jb.nfreq; f += blockDim.x) {
-        double ph = reduce_phase(dmul(dmul((double)n, dt), jb.omega[f]));
-        double s, c;
-        sincos(ph, &s, &c);
-        double add_re = dsub(dmul(c, o.x), dmul(s, o.y));
-        double add_im = dadd(dmul(c, o.y), dmul(s, o.x));
-        double2 sum = jb.acc[2 * f], comp = jb.acc[2 * f + 1];
-        double yr = dsub(add_re, comp.x), yi = dsub(add_im, comp.y);
-        double tr = dadd(sum.x, yr), ti = dadd(sum.y, yi);
-        comp.x = dsub(dsub(tr, sum.x), yr);
-        comp.y = dsub(dsub(ti, sum.y), yi);
-        jb.acc[2 * f] = make_double2(tr, ti);
-        jb.acc[2 * f + 1] = comp;
-    }
+    // one thread per frequency
+    for (int f = threadIdx.x; f < jb.nfreq; f += blockDim.x) accumulate_frequency(jb, f, o, dt, n);
+}
+
+__global__ void k_overlap_finalize(const OverlapJob *jobs, int njobs, const double2 *partials, int nparts,
+                                   double scale, double dt, const long long *step, int step_offset)
+{
+    const int jid = blockIdx.x;
+    if (jid >= njobs) return;
+    const OverlapJob jb = jobs[jid];
+    overlap_finalize_job(jb, partials + (long long)jid * nparts, nparts, scale, dt, *step + step_offset);
 }
 
 // ---------------------------------------------------------------------------
-// Running single-frequency DFT (timefield3d.c:2851-2975): acc += f * twiddle,
-// complex double per component; the twiddle is the host-computed
-// e^{i reduced phase} of the reference's power series.  Either the y-slice
-// j = slice (acc indexed [m][k][i]) or the whole grid (acc indexed [m][q]).
+// End of one step of a run, in one launch: blocks [0, njobs*nparts) compute
+// the overlap partials of the fields just updated, the next `src_blocks`
+// write the scheduled source plane of the NEXT step (step counter + 1).  The
+// last block to finish (completion count, after a memory fence) adds the
+// partials of every job in order -- the order of k_overlap_finalize, so the
+// monitors are bit-identical to the separate kernels -- accumulates the
+// frequencies, advances the step counter and resets the count for the next
+// launch.  Nothing waits on anything: blocks only count themselves out.
 // ---------------------------------------------------------------------------
+constexpr int kTailJobs = 64;
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_step_tail(TailArgs a)
+{
+    const int nov = a.njobs * a.nparts;
+    const int b = blockIdx.x;
+    if (b < nov) {
+        const int jid = b / a.nparts, part = b - jid * a.nparts;
+        const OverlapJob jb = a.jobs[jid];
+        overlap_block<T>((const T *const *)a.f, a.nx, a.ny, jb, part, a.nparts, a.partials + b);
+    } else {
+        double A, c, s;
+        schedule_values(a.src, *a.step + 1, A, c, s);
+        mode_source_cells(a.src, (b - nov) * (long long)blockDim.x + threadIdx.x,
+                          (long long)a.src_blocks * blockDim.x, A, c, s);
+    }
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(a.done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const long long n = *a.step;
+    // stage every partial in shared memory, then one thread per job adds its
+    // partials in order (the order of k_overlap_finalize)
+    constexpr int kStage = 1024;
+    __shared__ double2 part[kStage];
+    __shared__ double2 tot[kTailJobs];
+    const int np = a.njobs * a.nparts;
+    const bool staged = np <= kStage && a.njobs <= kTailJobs;
+    if (staged) {
+        for (int i = threadIdx.x; i < np; i += blockDim.x) part[i] = a.partials[i];
+        __syncthreads();
+        if (threadIdx.x < a.njobs) {
+            const int jid = threadIdx.x;
+            double sre = 0.0, sim = 0.0;
+            for (int p = 0; p < a.nparts; p++) {
+                const double2 v = part[jid * a.nparts + p];
+                sre = dadd(sre, v.x);
+                sim = dadd(sim, v.y);
+            }
+            tot[jid] = make_double2(dmul(a.scale, sre), dmul(a.scale, sim));
+            const OverlapJob jb = a.jobs[jid];
+            if (jb.inst) *jb.inst = tot[jid];
+        }
+        __syncthreads();
+        // one thread per (job, frequency)
+        for (int jid = 0; jid < a.njobs; jid++) {
+            const OverlapJob jb = a.jobs[jid];
+            if (!jb.acc) continue;
+            for (int f = threadIdx.x; f < jb.nfreq; f += blockDim.x) accumulate_frequency(jb, f, tot[jid], a.dt, n);
+        }
+    } else {
+        for (int jid = 0; jid < a.njobs; jid++) {
+            const OverlapJob jb = a.jobs[jid];
+            overlap_finalize_job(jb, a.partials + (long long)jid * a.nparts, a.nparts, a.scale, a.dt, n);
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *a.step = n + 1;
+        *a.done = 0u;
+    }
+}
+
 template <typename T>
 __global__ void k_dft(const T *const *f, int nx, int ny, int nz, int slice, int k_lo, int k_hi, double tr,
                       double ti, double2 *acc)
@@ -271,19 +370,49 @@ __global__ void k_check_finite(const float *a, long long n, int *bad)
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
+static int source_blocks(int nx, int ny)
+{
+    long long nxy = (long long)nx * ny;
+    int blocks = (int)((nxy + 255) / 256);
+    return blocks > 1184 ? 1184 : blocks;
+}
+
 void launch_mode_source(float *plane, const float *const ep_plane[3], const float *const mu_plane[3], int nx, int ny,
                         int cx, int cy, const double2 *mode, int mi, int mj, double ratio, double amplitude,
                         double cph, double sph, const double *sched, const long long *step, int nsched, int reverse,
                         int adjoint, cudaStream_t st)
 {
-    long long nxy = (long long)nx * ny;
-    int blocks = (int)((nxy + 255) / 256);
-    if (blocks > 1184) blocks = 1184;
-    note_launch();
-    k_mode_source<<<blocks, 256, 0, st>>>(plane, ep_plane[0], ep_plane[1], ep_plane[2], mu_plane[0], mu_plane[1],
-                                          mu_plane[2], nx, ny, cx, cy, mode, mi, mj, ratio, amplitude, cph, sph, sched,
-                                          step, nsched, reverse, adjoint);
+    SourceJob sj{};
+    sj.plane = plane;
+    for (int c = 0; c < 3; c++) { sj.ep[c] = ep_plane[c]; sj.mu[c] = mu_plane[c]; }
+    sj.nx = nx; sj.ny = ny; sj.cx = cx; sj.cy = cy;
+    sj.mode = mode; sj.mi = mi; sj.mj = mj; sj.ratio = ratio;
+    sj.sched = sched; sj.nsched = nsched; sj.reverse = reverse; sj.adjoint = adjoint;
+    launch_mode_source_job(sj, amplitude, cph, sph, step, 0, st);
 }
+
+void launch_mode_source_job(const SourceJob &sj, double amplitude, double cph, double sph, const long long *step,
+                            int step_offset, cudaStream_t st)
+{
+    note_launch();
+    k_mode_source<<<source_blocks(sj.nx, sj.ny), 256, 0, st>>>(sj, amplitude, cph, sph, step, step_offset);
+}
+
+template <typename T>
+void launch_step_tail(TailArgs a, cudaStream_t st)
+{
+    a.nparts = overlap_parts(a.nx, a.ny);
+    a.src_blocks = a.src.plane ? source_blocks(a.src.nx, a.src.ny) : 0;
+    const int blocks = a.njobs * a.nparts + a.src_blocks;
+    note_launch();
+    if (blocks == 0) {
+        k_step_advance<<<1, 1, 0, st>>>(a.step);
+        return;
+    }
+    k_step_tail<T><<<blocks, 256, 0, st>>>(a);
+}
+template void launch_step_tail<float>(TailArgs, cudaStream_t);
+template void launch_step_tail<double>(TailArgs, cudaStream_t);
 
 void launch_set_value(float *p, long long idx, float v, cudaStream_t st)
 {

@@ -341,7 +341,7 @@ Grid::~Grid()
         for (int m = 0; m < 6; m++) dfree(sig[m]);
         for (auto &p : planes) dfree(p.p);
         for (auto p : plane_pool) dfree(p);
-        dfree(d_step); dfree(d_jobs); dfree(d_job1); dfree(d_partials); dfree(d_inst);
+        dfree(d_step); dfree(d_done); dfree(d_jobs); dfree(d_job1); dfree(d_partials); dfree(d_inst);
         if (h_inst) cudaFreeHost(h_inst);
         if (h_flag) cudaFreeHost(h_flag);
         if (h_err) cudaFreeHost(h_err);
@@ -534,6 +534,7 @@ bool grid_ensure_device(Grid *g)
         for (int m = 0; m < 6; m++)
             if (!dalloc(&g->sig[m], fb, g->st, false)) return false;
         if (!dalloc(&g->d_step, sizeof(long long), g->st)) return false;
+        if (!dalloc(&g->d_done, sizeof(unsigned), g->st)) return false;
         if (!dalloc(&g->d_flag, 12 * sizeof(int), g->st)) return false;
         CK(cudaMallocHost(&g->h_flag, 12 * sizeof(int)));
         CK(cudaMallocHost(&g->h_inst, sizeof(double2)));
@@ -885,6 +886,8 @@ static bool step_fused(Grid *g, double dt)
     return true;
 }
 
+static bool schedule_job(Grid *g, SourceJob *sj);
+
 bool enqueue_after_step(Grid *g, double dt)
 {
     const void *const *fp = (const void *const *)g->d_fptr[g->cur];
@@ -893,8 +896,8 @@ bool enqueue_after_step(Grid *g, double dt)
         if (f64) launch_probes<double>((const double *const *)fp, g->d_probes, (int)g->probes.size(), g->d_probe_buf, g->probe_cap, g->d_probe_count, g->st);
         else launch_probes<float>((const float *const *)fp, g->d_probes, (int)g->probes.size(), g->d_probe_buf, g->probe_cap, g->d_probe_count, g->st);
     }
-    if (g->njobs > 0) {
-        double scale = (-0.5 * g->dx * g->dx);
+    const double scale = (-0.5 * g->dx * g->dx);
+    if (g->njobs > 0 && !g->in_run) {
         if (f64) launch_overlap<double>((const double *const *)fp, g->nx, g->ny, g->d_jobs, g->njobs, g->d_partials, scale, dt, g->d_step, 0, g->st);
         else launch_overlap<float>((const float *const *)fp, g->nx, g->ny, g->d_jobs, g->njobs, g->d_partials, scale, dt, g->d_step, 0, g->st);
     }
@@ -906,7 +909,22 @@ bool enqueue_after_step(Grid *g, double dt)
         if (!td) continue;
         if (!enqueue_taper_store(td, g, b.which, 0, g->d_step, b.t0, b.dir)) return false;
     }
-    launch_step_advance(g->d_step, g->st);
+    if (!g->in_run) {
+        launch_step_advance(g->d_step, g->st);
+    } else {
+        // overlaps of this step, scheduled source of the next, counter: one launch
+        TailArgs t{};
+        t.f = fp;
+        t.nx = g->nx; t.ny = g->ny;
+        t.jobs = g->d_jobs; t.njobs = g->njobs;
+        t.partials = g->d_partials;
+        t.scale = scale; t.dt = dt;
+        t.step = g->d_step;
+        t.done = g->d_done;
+        if (g->sched.active && !schedule_job(g, &t.src)) return false;
+        if (f64) launch_step_tail<double>(t, g->st);
+        else launch_step_tail<float>(t, g->st);
+    }
     CKL("after step");
     return true;
 }
@@ -936,22 +954,40 @@ bool rebuild_jobs(Grid *g)
     return true;
 }
 
+// the scheduled source as a SourceJob (its plane must exist)
+static bool schedule_job(Grid *g, SourceJob *sj)
+{
+    auto it = priv_modes().find(g->sched.mode_key);
+    Plane *pl = grid_plane(g, g->sched.cz, false);
+    if (it == priv_modes().end() || !pl) {
+        set_error(FDTD_ERR_ARG, "scheduled source not prepared");
+        return false;
+    }
+    const long long off = (long long)g->nx * g->ny * g->sched.cz;
+    *sj = SourceJob{};
+    sj->plane = pl->p;
+    for (int c = 0; c < 3; c++) { sj->ep[c] = g->ep[c] + off; sj->mu[c] = g->mu[c] + off; }
+    sj->nx = g->nx; sj->ny = g->ny; sj->cx = g->sched.cx; sj->cy = g->sched.cy;
+    sj->mode = it->second.d; sj->mi = it->second.mi; sj->mj = it->second.mj;
+    sj->ratio = g->dx / it->second.disc;
+    sj->sched = g->sched.d_sched; sj->nsched = g->sched.n;
+    sj->reverse = g->sched.reverse; sj->adjoint = g->sched.adjoint;
+    return true;
+}
+
+// write the scheduled source of step (counter + offset)
+static bool enqueue_schedule(Grid *g, int offset)
+{
+    SourceJob sj;
+    if (!schedule_job(g, &sj)) return false;
+    launch_mode_source_job(sj, 0, 0, 0, g->d_step, offset, g->st);
+    return true;
+}
+
 bool enqueue_step(Grid *g, double dt, bool with_extras)
 {
-    if (g->sched.active) {
-        auto it = priv_modes().find(g->sched.mode_key);
-        Plane *pl = grid_plane(g, g->sched.cz, false);
-        if (it == priv_modes().end() || !pl) {
-            set_error(FDTD_ERR_ARG, "scheduled source not prepared");
-            return false;
-        }
-        const long long nxy = (long long)g->nx * g->ny, off = nxy * g->sched.cz;
-        const float *epp[3] = {g->ep[0] + off, g->ep[1] + off, g->ep[2] + off};
-        const float *mup[3] = {g->mu[0] + off, g->mu[1] + off, g->mu[2] + off};
-        launch_mode_source(pl->p, epp, mup, g->nx, g->ny, g->sched.cx, g->sched.cy, it->second.d, it->second.mi,
-                           it->second.mj, g->dx / it->second.disc, 0, 0, 0, g->sched.d_sched, g->d_step, g->sched.n,
-                           g->sched.reverse, g->sched.adjoint, g->st);
-    }
+    // inside a run the previous step's tail kernel wrote this step's source
+    if (g->sched.active && !g->in_run && !enqueue_schedule(g, 0)) return false;
     bool ok;
     // External: captured as an event-record node whose timestamp the host can
     // read after a replay (a plain record during capture is only a dependency)
@@ -1055,10 +1091,26 @@ bool drain_kernel_timing(Grid *g, int set)
     return true;
 }
 
+static bool run_steps_in(Grid *g, double dt, int nsteps);
+
 bool run_steps(Grid *g, double dt, int nsteps)
 {
     if (nsteps <= 0) return true;
     if (!prepare_run(g, dt)) return false;
+    // Each step of a run ends with the step-tail kernel, which also writes the
+    // next step's scheduled source: prime the first one here, and afterwards
+    // leave the plane holding the last step's source, as a stepwise loop would.
+    if (g->sched.active && !enqueue_schedule(g, 0)) return false;
+    g->in_run = true;
+    const bool ok = run_steps_in(g, dt, nsteps);
+    g->in_run = false;
+    if (!ok) return false;
+    if (g->sched.active && !enqueue_schedule(g, -1)) return false;
+    return true;
+}
+
+static bool run_steps_in(Grid *g, double dt, int nsteps)
+{
     int full = nsteps / kGraphSteps, rest = nsteps % kGraphSteps;
     if (full > 0 && !g->ktime) {
         if (!capture_graph(g, 0, dt)) return false;

@@ -24,6 +24,35 @@ struct OverlapJob {
     int nfreq;
 };
 
+// plane source written from a complex mode (timefield3d_mode_source and
+// its adjoint); sched != null: per-step (amplitude, cos, sin) triples
+struct SourceJob {
+    float *plane;               // 6 components of nx*ny
+    const float *ep[3], *mu[3]; // material of the source plane
+    int nx, ny, cx, cy;
+    const double2 *mode;
+    int mi, mj;
+    double ratio;
+    const double *sched;
+    int nsched;
+    int reverse, adjoint;
+};
+
+// one launch at the end of a run step: overlap monitors of the step, the
+// scheduled source of the next step (src.plane != null) and the step counter
+struct TailArgs {
+    const void *const *f;       // device array of the 6 field pointers
+    int nx, ny;
+    const OverlapJob *jobs;
+    int njobs, nparts;
+    double2 *partials;
+    double scale, dt;
+    long long *step;
+    SourceJob src;
+    int src_blocks;
+    unsigned *done;             // completion count, 0 between launches
+};
+
 struct ProbeJob {
     long long q;
     int m;
@@ -111,6 +140,10 @@ void launch_mode_source(float *plane, const float *const ep_plane[3], const floa
                         int cx, int cy, const double2 *mode, int mi, int mj, double ratio, double amplitude,
                         double cph, double sph, const double *sched, const long long *step, int nsched, int reverse,
                         int adjoint, cudaStream_t st);
+void launch_mode_source_job(const SourceJob &sj, double amplitude, double cph, double sph, const long long *step,
+                            int step_offset, cudaStream_t st);
+template <typename T>
+void launch_step_tail(TailArgs a, cudaStream_t st);
 void launch_set_value(float *p, long long idx, float v, cudaStream_t st);
 int overlap_parts(int nx, int ny);
 template <typename T>

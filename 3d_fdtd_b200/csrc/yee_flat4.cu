@@ -443,7 +443,7 @@ __global__ void __launch_bounds__(kBlock4, W == 4 ? (SLABS ? 2 : 4) : 3) k_flat4
 //   planes L..nz-L-1: nb_box box blocks (W 4, plain), nb_y y-slab-row blocks
 //   (W 2, SLABS 2), nb_x x-slab-column blocks (W 2, SLABS 3)
 template <bool E_FIELD, bool LOSSY>
-__global__ void __launch_bounds__(kBlock4, 3) k_flat4_merged(FlatArgs a, Plan4 p)
+__global__ void __launch_bounds__(kBlock4, E_FIELD ? 3 : 4) k_flat4_merged(FlatArgs a, Plan4 p)
 {
     int b = blockIdx.x;
     const int nzs = (p.L - 1) * p.nbz, nmb = p.nmid * p.nbm;

@@ -153,6 +153,7 @@ SIGNATURES = {
     "adjoint3d_taper_sync_host": (i, [P]),
     "fdtd_set_device": (i, [i]),
     "fdtd_launch_count": (ll, []),
+    "fdtd_wait_selftest": (i, [d, dp]),
     "timefield3d_get_stream": (C.c_void_p, [T]),
     "timefield3d_upload_materials": (i, [T]),
     "timefield3d_set_kernel_timing": (i, [T, i]),

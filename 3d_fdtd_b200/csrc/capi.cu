@@ -1183,6 +1183,44 @@ int fdtd_set_device(int device)
 
 long long fdtd_launch_count(void) { return launch_count(); }
 
+int fdtd_wait_selftest(double limit_seconds, double *elapsed_seconds)
+{
+    LOCK;
+    if (!device_available()) return fdtd_last_error();
+    if (!(limit_seconds > 0.0) || limit_seconds > 10.0) {
+        set_error(FDTD_ERR_ARG, "wait self-test limit %g s: must be in (0, 10]", limit_seconds);
+        return FDTD_ERR_ARG;
+    }
+    cudaStream_t st = nullptr;
+    int *d_err = nullptr;
+    unsigned long long *d_el = nullptr;
+    int h_err = 0;
+    unsigned long long h_el = 0;
+    bool ok = cuda_ok(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate") &&
+              cuda_ok(cudaMalloc(&d_err, sizeof(int)), "cudaMalloc") &&
+              cuda_ok(cudaMalloc(&d_el, sizeof(unsigned long long)), "cudaMalloc") &&
+              cuda_ok(cudaMemsetAsync(d_err, 0, sizeof(int), st), "cudaMemsetAsync");
+    if (ok) {
+        launch_wait_selftest((unsigned long long)(limit_seconds * 1e9), d_err, d_el, st);
+        ok = cuda_ok(cudaGetLastError(), "wait self-test launch") &&
+             cuda_ok(cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync") &&
+             cuda_ok(cudaMemcpyAsync(&h_el, d_el, sizeof(h_el), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync") &&
+             cuda_ok(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    }
+    if (d_err) cudaFree(d_err);
+    if (d_el) cudaFree(d_el);
+    if (st) cudaStreamDestroy(st);
+    if (!ok) return fdtd_last_error();
+    if (elapsed_seconds) *elapsed_seconds = (double)h_el * 1e-9;
+    if (h_err) {
+        set_error(FDTD_ERR_TIMEOUT, "wait self-test: the bounded wait gave up after %.3f s as designed",
+                  (double)h_el * 1e-9);
+        return FDTD_ERR_TIMEOUT;
+    }
+    set_error(FDTD_ERR_CUDA, "wait self-test: a wait on a barrier nothing arrives on completed");
+    return FDTD_ERR_CUDA;
+}
+
 void *timefield3d_get_stream(timefield3d psi)
 {
     LOCK;

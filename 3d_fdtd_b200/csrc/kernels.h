@@ -134,6 +134,7 @@ int fused_tma_supported(int nx, int ny, int nz);
 bool fused_make_maps(FusedMaps *m, const float *const f[6], const float *const cb[3], const float *const ca[3],
                      int nx, int ny, int nz);
 void launch_fused_step_tma(const FusedArgs &a, const FusedMaps &m, int *err, cudaStream_t st);
+void launch_wait_selftest(unsigned long long limit_ns, int *err, unsigned long long *elapsed_ns, cudaStream_t st);
 
 // aux_kernels.cu
 void launch_mode_source(float *plane, const float *const ep_plane[3], const float *const mu_plane[3], int nx, int ny,

@@ -126,13 +126,15 @@ __device__ __forceinline__ void xslab_load(XSlab<W> &x, const FlatArgs &a, int g
 template <int W, int A0, int SLABS>
 __device__ __forceinline__ void xslab_store(const XSlab<W> &x, const FlatArgs &a, int g)
 {
-    if (!(SLABS & 1) || !x.any) return;
+    if constexpr ((SLABS & 1) != 0) {
+        if (!x.any) return;
 #pragma unroll
-    for (int e = 0; e < W; e++) {
-        if (!x.valid[e]) continue;
-        const long long s = x.s0 + slab_local(W * g + e, a.nx, a.L);
-        a.psi[0][A0][s] = x.p0[e];
-        a.psi[0][A0 + 1][s] = x.p1[e];
+        for (int e = 0; e < W; e++) {
+            if (!x.valid[e]) continue;
+            const long long s = x.s0 + slab_local(W * g + e, a.nx, a.L);
+            a.psi[0][A0][s] = x.p0[e];
+            a.psi[0][A0 + 1][s] = x.p1[e];
+        }
     }
 }
 

@@ -24,10 +24,11 @@
 // the cp.async kernel); shared-memory destinations are 128-byte aligned and the
 // kernel checks that before issuing any copy.  Loads only, no multicast.
 //
-// Waits on the mbarriers are bounded.  A wait that gives up sets the grid's
-// device error flag and a block-wide abort flag; the block then finishes its
-// loop without waiting (results are garbage, the host reports
-// FDTD_ERR_TIMEOUT) instead of hanging.
+// Waits on the mbarriers are bounded in time (kWaitNs of %globaltimer).  A
+// wait that gives up sets the grid's device error flag and a block-wide abort
+// flag; the block then finishes its loop without waiting (results are
+// garbage, the host reports FDTD_ERR_TIMEOUT) instead of hanging.
+// k_wait_selftest runs the same bounded wait on a barrier nothing arrives on.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -40,7 +41,7 @@ constexpr int TX = 32;
 constexpr int HW = TX + 8;   // H box width: x from X0-4 to X0+TX+3
 constexpr int EW = TX + 4;   // E / coefficient box width: x from X0 to X0+TX+3
 constexpr int HOFF = 4;      // box x index of tile column 0 in an H box
-constexpr unsigned kWaitLimit = 1u << 22;
+constexpr unsigned long long kWaitNs = 1000000000ull;   // 1 s: a plane's loads take microseconds
 
 constexpr int pad128f(int nfloats) { return ((nfloats * 4 + 127) / 128) * 32; }
 
@@ -92,6 +93,27 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
     return ok != 0;
 }
 
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// true when the barrier's phase `parity` completed; false when *abort was set
+// by another thread or limit_ns passed
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity,
+                                                  unsigned long long limit_ns, volatile int *abort)
+{
+    const unsigned long long t0 = global_ns();
+    for (;;) {
+        if (*abort) return false;   // checked first: after a refused start the barriers were never set up
+        if (mbar_try_wait(bar, parity)) return true;
+        // try_wait may suspend for a hardware-defined while: check the clock every time
+        if (global_ns() - t0 > limit_ns) return false;
+    }
+}
+
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z,
                                             unsigned long long *bar)
 {
@@ -141,10 +163,7 @@ __device__ __forceinline__ void wait_plane(TmaSmem<TY, LOSSY> &sm, int k, int z0
     const int slot = (k + 3) % 3;
     const unsigned parity = (unsigned)(((k - z0 + 1) / 3) & 1);
     volatile int *abort = &sm.abort;
-    for (unsigned it = 0; it < kWaitLimit; it++) {
-        if (*abort) return;   // checked first: after a refused start the barriers were never set up
-        if (mbar_try_wait(&sm.bar[slot], parity)) return;
-    }
+    if (mbar_wait_bounded(&sm.bar[slot], parity, kWaitNs, abort) || *abort) return;
     *abort = 1;
     atomicExch(err, 1);
 }
@@ -574,6 +593,34 @@ void launch_fused_step_tma(const FusedArgs &a, const FusedMaps &m, int *err, cud
         if (lossy) launch_tma<false, true>(a, m, err, st);
         else launch_tma<false, false>(a, m, err, st);
     }
+}
+
+// Self-test of the bounded wait: one block waits on an mbarrier that expects
+// one arrival which never comes.  The wait must give up after limit_ns, set
+// *err like a pipeline wait does and leave the kernel (and the context) in
+// good order; *elapsed_ns records how long it waited.
+__global__ void k_wait_selftest(unsigned long long limit_ns, int *err, unsigned long long *elapsed_ns)
+{
+    __shared__ unsigned long long bar;
+    __shared__ int abort;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        abort = 0;
+    }
+    __syncthreads();
+    const unsigned long long t0 = global_ns();
+    const bool done = mbar_wait_bounded(&bar, 0, limit_ns, &abort);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (!done) atomicExch(err, 1);
+        *elapsed_ns = global_ns() - t0;
+    }
+}
+
+void launch_wait_selftest(unsigned long long limit_ns, int *err, unsigned long long *elapsed_ns, cudaStream_t st)
+{
+    note_launch();
+    k_wait_selftest<<<1, 32, 0, st>>>(limit_ns, err, elapsed_ns);
 }
 
 }  // namespace fdtd

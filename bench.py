@@ -290,25 +290,8 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
         raise SystemExit("bench: no CUDA device")
     torch.cuda.set_device(local_rank)
     fd.call("fdtd_set_device", local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = importlib.import_module("3d_fdtd_b200.replicas").Ranks("nccl", timeout_s=120)
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     sim = Taper(fd, args.time_steps, {"auto": 0, "flat": 1, "fused": 2, "flat4": 3}[args.yee_variant])
     stream = torch.cuda.ExternalStream(fd.lib.timefield3d_get_stream(sim.t))
@@ -385,9 +368,7 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
                 "transmission": {"lambda_um": W["lams"], "T": [round(float(x), 6) for x in trans],
                                  "T_e2e_equal": bool(np.allclose(trans, trans_e2e, rtol=1e-6))}}
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
 
 
 def main():

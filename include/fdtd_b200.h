@@ -296,6 +296,12 @@ int timefield3d_release_mode(mode m);
 int fdtd_set_device(int device);
 /* kernels this library has launched so far (graph replays counted per kernel) */
 long long fdtd_launch_count(void);
+/* Self-test of the engine's bounded device waits (no reference counterpart):
+ * one block waits, with the routine the TMA pipeline uses, on a barrier that
+ * nothing arrives on.  Expected result FDTD_ERR_TIMEOUT after about
+ * limit_seconds (0 < limit <= 10), reported like a real pipeline timeout, with
+ * the CUDA context still usable; *elapsed_seconds = the device-side wait. */
+int fdtd_wait_selftest(double limit_seconds, double *elapsed_seconds);
 /* the grid's CUDA stream (cudaStream_t), for callers that order work or time it */
 void *timefield3d_get_stream(timefield3d psi);
 /* upload psi.ep/mu/sig now (otherwise done on the next device use after a change) */

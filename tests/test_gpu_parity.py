@@ -340,3 +340,19 @@ def test_run_graph_equals_stepwise(fd, gpu):
     assert np.array_equal(outs[0][0], outs[1][0])
     assert np.array_equal(outs[0][1], outs[1][1])
     assert np.abs(outs[0][1]).max() > 0
+
+
+def test_bounded_wait_times_out_and_context_survives(fd, gpu):
+    """A device wait on a barrier nothing arrives on gives up after its limit,
+    reports FDTD_ERR_TIMEOUT like a pipeline timeout, and the GPU keeps working."""
+    el = C.c_double()
+    r = fd.lib.fdtd_wait_selftest(0.05, C.byref(el))
+    assert r == fd.FDTD_ERR_TIMEOUT, fd.lib.fdtd_last_error_message()
+    assert 0.05 <= el.value < 1.0, el.value
+    fd.lib.fdtd_clear_error()
+    # the context is still usable: a small FP64 run completes without error
+    grid = fd.Grid(12, 12, 12, 0.02)
+    fd.call("timefield3d_set_source_value", grid.t, 6, 6, 6, 2, 1.0)
+    fd.call("timefield3d_run", grid.t, DT_FACTOR * 0.02, 10)
+    fd.call("timefield3d_synchronize", grid.t)
+    assert np.abs(grid.fields()).max() > 0

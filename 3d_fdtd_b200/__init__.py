@@ -154,6 +154,9 @@ SIGNATURES = {
     "fdtd_set_device": (i, [i]),
     "fdtd_launch_count": (ll, []),
     "fdtd_wait_selftest": (i, [d, dp]),
+    "fdtd_mode_solve_beta_squared": (Complex, [C.POINTER(Mode), d, d, C.POINTER(Mode), i, i, i, i]),
+    "fdtd_mode_solve_restarts": (i, []),
+    "fdtd_mode_apply_beta_squared": (i, [Mode, d, Mode]),
     "timefield3d_get_stream": (C.c_void_p, [T]),
     "timefield3d_upload_materials": (i, [T]),
     "timefield3d_set_kernel_timing": (i, [T, i]),

@@ -1183,6 +1183,64 @@ int fdtd_set_device(int device)
 
 long long fdtd_launch_count(void) { return launch_count(); }
 
+namespace {
+bool mode_ok(const mode *m, const char *what)
+{
+    if (!m || m->i < 3 || m->j < 3 || !m->fields.m || !m->ep.m || !m->mu.m || !m->pml.m || !(m->disc > 0)) {
+        set_error(FDTD_ERR_ARG, "%s: mode must be at least 3 x 3 with disc > 0 and all arrays allocated", what);
+        return false;
+    }
+    return true;
+}
+int last_mode_restarts = 0;
+}  // namespace
+
+int fdtd_mode_apply_beta_squared(mode in, double omega, mode out)
+{
+    LOCK;
+    if (!device_available()) return fdtd_last_error();
+    if (!mode_ok(&in, "fdtd_mode_apply_beta_squared") || !mode_ok(&out, "fdtd_mode_apply_beta_squared"))
+        return FDTD_ERR_ARG;
+    if (out.i != in.i || out.j != in.j) {
+        set_error(FDTD_ERR_ARG, "fdtd_mode_apply_beta_squared: output %dx%d, input %dx%d", out.i, out.j, in.i, in.j);
+        return FDTD_ERR_ARG;
+    }
+    return mode_apply_beta2_device(in, omega, out) ? FDTD_OK : fdtd_last_error();
+}
+
+complex fdtd_mode_solve_beta_squared(mode *psi, double omega, double tol, mode *prev_modes, int prev_num, int size,
+                                     int confinement, int lateral_symmetry)
+{
+    LOCK;
+    complex zero{0.0, 0.0};
+    last_mode_restarts = 0;
+    if (!device_available()) return zero;
+    if (!mode_ok(psi, "fdtd_mode_solve_beta_squared")) return zero;
+    if (!(omega > 0) || !(tol > 0) || size < 2 || size > 512 || (confinement != 1 && confinement != 2) ||
+        prev_num < 0 || (prev_num > 0 && !prev_modes)) {
+        set_error(FDTD_ERR_ARG, "fdtd_mode_solve_beta_squared: omega %g tol %g size %d confinement %d prev_num %d",
+                  omega, tol, size, confinement, prev_num);
+        return zero;
+    }
+    for (int p = 0; p < prev_num; p++) {
+        if (!mode_ok(&prev_modes[p], "fdtd_mode_solve_beta_squared (previous mode)")) return zero;
+        if (prev_modes[p].i != psi->i || prev_modes[p].j != psi->j) {
+            set_error(FDTD_ERR_ARG, "fdtd_mode_solve_beta_squared: previous mode %d is %dx%d, mode %dx%d", p,
+                      prev_modes[p].i, prev_modes[p].j, psi->i, psi->j);
+            return zero;
+        }
+    }
+    std::complex<double> beta;
+    int restarts = 0;
+    if (!mode_solve_device(psi, omega, tol, prev_modes, prev_num, size, confinement, lateral_symmetry, 5000, &beta,
+                           &restarts))
+        return zero;
+    last_mode_restarts = restarts;
+    return complex{beta.real(), beta.imag()};
+}
+
+int fdtd_mode_solve_restarts(void) { return last_mode_restarts; }
+
 int fdtd_wait_selftest(double limit_seconds, double *elapsed_seconds)
 {
     LOCK;

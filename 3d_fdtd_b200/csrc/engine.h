@@ -6,6 +6,7 @@
 // `fields.m`.
 #pragma once
 
+#include <complex>
 #include <cstdint>
 #include <map>
 #include <memory>
@@ -17,6 +18,11 @@
 #include "kernels.h"
 
 namespace fdtd {
+
+// ---- mode solver (mode_solver.cu) --------------------------------------------
+bool mode_apply_beta2_device(const mode &in, double omega, mode &out);
+bool mode_solve_device(mode *psi, double omega, double tol, const mode *prev, int nprev, int size, int confinement,
+                       int lateral_symmetry, int max_restarts, std::complex<double> *beta_out, int *restarts_out);
 
 // ---- status ----------------------------------------------------------------
 void set_error(int code, const char *fmt, ...);

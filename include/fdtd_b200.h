@@ -296,6 +296,25 @@ int timefield3d_release_mode(mode m);
 int fdtd_set_device(int device);
 /* kernels this library has launched so far (graph replays counted per kernel) */
 long long fdtd_launch_count(void);
+/* Waveguide eigenmode on the GPU in FP64: the reference's restarted Arnoldi
+ * beta^2 solver, mode_solve_beta_squared (mode.c:3461-3616), same arguments
+ * and meaning; fills psi->fields (6 components, H-normalised) and returns
+ * beta.  A different name because the reference's mode.o, which a program
+ * keeps linking for mode_new and friends, already defines the original.
+ * Starts from the reference's rand() vector; stops, like the reference, when
+ * |n_eff| changes by less than tol between restarts (at most 5000 restarts,
+ * else FDTD_ERR_TIMEOUT).  On failure returns 0 with the status set. */
+complex fdtd_mode_solve_beta_squared(mode *psi, double omega, double tol, mode *prev_modes, int prev_num, int size,
+                                     int confinement, int lateral_symmetry);
+/* restarts the last fdtd_mode_solve_beta_squared took (no reference counterpart) */
+int fdtd_mode_solve_restarts(void);
+/* One application of the beta^2 operator, mode_apply_beta_squared_operator
+ * (mode.c:2796-2943), on the GPU: out.fields = B in.fields (Hx, Hy on interior
+ * cells; every other entry 0).  The reference returns a new mode with in's
+ * materials; here the caller passes `out` of the same size (its ep/mu/pml are
+ * not touched).  Bit-identical to the reference for the same input. */
+int fdtd_mode_apply_beta_squared(mode in, double omega, mode out);
+
 /* Self-test of the engine's bounded device waits (no reference counterpart):
  * one block waits, with the routine the TMA pipeline uses, on a barrier that
  * nothing arrives on.  Expected result FDTD_ERR_TIMEOUT after about

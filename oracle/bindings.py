@@ -95,6 +95,11 @@ class Reference:
             "mode_smul": (None, [Complex, M]),
             "mode_power_normalize": (None, [M]),
             "mode_power_norm": (d, [M]),
+            "mode_set_background": (None, [M, Complex, Complex]),
+            "mode_make_rectangle": (None, [M, Complex, Complex, i, i, i, i]),
+            "mode_set_pml": (None, [M, d, i, i]),
+            "mode_apply_beta_squared_operator": (M, [M, d]),
+            "mode_solve_beta_squared": (Complex, [C.POINTER(M), d, d, C.POINTER(M), i, i, i, i]),
             "complex_exp": (Complex, [Complex]),
             "adjoint3d_taper_new": (P, [d, d, i, i, i, C.POINTER(i), C.POINTER(i), i, i, i]),
             "adjoint3d_taper_insert": (None, [T, P]),

@@ -157,6 +157,13 @@ SIGNATURES = {
     "fdtd_mode_solve_beta_squared": (Complex, [C.POINTER(Mode), d, d, C.POINTER(Mode), i, i, i, i]),
     "fdtd_mode_solve_restarts": (i, []),
     "fdtd_mode_apply_beta_squared": (i, [Mode, d, Mode]),
+    "fdtd_spline_basis": (i, [i, i, i, dp]),
+    "timefield3d_set_spline_taper": (i, [T, d, d, i, dp, d, i, i, i, i]),
+    "fdtd_spline_store_new": (C.c_void_p, [T, i, dp, d, i, i, i, i, i]),
+    "fdtd_spline_store_bind": (i, [C.c_void_p, T, i, i, i]),
+    "fdtd_spline_store_unbind": (i, [C.c_void_p, T]),
+    "fdtd_spline_store_gradient": (i, [C.c_void_p, d, dp, dp]),
+    "fdtd_spline_store_free": (None, [C.c_void_p]),
     "timefield3d_get_stream": (C.c_void_p, [T]),
     "timefield3d_upload_materials": (i, [T]),
     "timefield3d_set_kernel_timing": (i, [T, i]),

@@ -315,6 +315,35 @@ int fdtd_mode_solve_restarts(void);
  * not touched).  Bit-identical to the reference for the same input. */
 int fdtd_mode_apply_beta_squared(mode in, double omega, mode out);
 
+/* ---- spline taper (no reference counterpart; generalises timefield3d_set_taper,
+ * timefield3d.c:1511-1535, and the taper gradient, adjoint3d.c:339-418) ------
+ * Width on plane k: natural cubic spline through `ncontrol` widths (um) placed
+ * evenly on [start_z, end_z - 1].  The core spans x in
+ * [center_x - w/(2 disc), center_x + w/(2 disc)) (cell units, cell i covers
+ * [i, i+1)) on rows [bottom, top); a cell covered by a fraction f gets
+ * ep_old + f (ep - ep_old) (mu alike, all 3 components), fully covered cells
+ * get ep exactly, so integer edges fill exactly like timefield3d_set_taper. */
+/* weights[(k - start_z) * ncontrol + c]: weight of width c in width(k) */
+int fdtd_spline_basis(int ncontrol, int start_z, int end_z, double *weights);
+/* rasterise (host arrays, and the device copy directly when it is current) */
+int timefield3d_set_spline_taper(timefield3d psi, double ep, double mu, int ncontrol, const double *widths,
+                                 double center_x, int start_z, int end_z, int bottom, int top);
+/* Edge store for the adjoint gradient of a spline taper: E at the cell holding
+ * each core edge, per row and plane ([k][j][edge], edge 0 right, 1 left), for
+ * `duration` steps, forward and adjoint, on the GPU.  Bind it to a grid like
+ * adjoint3d_taper_bind_store (which 0 forward / 1 adjoint; after step n of
+ * timefield3d_run it stores at t0 + dir*n); unbind before freeing. */
+typedef struct fdtd_spline_store_ *fdtd_spline_store;
+fdtd_spline_store fdtd_spline_store_new(timefield3d psi, int ncontrol, const double *widths, double center_x,
+                                        int start_z, int end_z, int bottom, int top, int duration);
+int fdtd_spline_store_bind(fdtd_spline_store store, timefield3d psi, int which, int t0, int dir);
+int fdtd_spline_store_unbind(fdtd_spline_store store, timefield3d psi);
+/* grad[c] = sum_k sum_j W[k][c] / (2 disc) (g_right + g_left) ep_diff with
+ * g = sum_t sum_m E_fwd E_adj at the edge cells; cell_gradient (optional,
+ * 2*(top-bottom)*(end_z-start_z) values) receives g */
+int fdtd_spline_store_gradient(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient);
+void fdtd_spline_store_free(fdtd_spline_store store);
+
 /* Self-test of the engine's bounded device waits (no reference counterpart):
  * one block waits, with the routine the TMA pipeline uses, on a barrier that
  * nothing arrives on.  Expected result FDTD_ERR_TIMEOUT after about

@@ -258,7 +258,7 @@ void timefield3d_free(timefield3d psi)
 {
     LOCK;
     Grid *g = grid_lookup(psi, true);
-    if (g && g->dev) {
+    if (g && g->mirrors_pinned) {
         cudaHostUnregister(psi.ep);
         cudaHostUnregister(psi.mu);
         cudaHostUnregister(psi.sig);

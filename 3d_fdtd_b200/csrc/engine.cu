@@ -436,6 +436,16 @@ bool grid_upload_materials(Grid *g)
     // only the arrays the rasterisers touched (kMatEp / kMatMu / kMatSig bits);
     // flags: [0..2] ep != 1, [3..5] mu != 1, [6..11] sig != 0 (bit 2: not finite)
     const int dirty = g->mat_dirty;
+    // Pin the host material mirrors once a grid uploads them a second time
+    // (design loops re-rasterise and re-upload every evaluation); a grid
+    // uploaded once does not pay for pinning (hundreds of ms per GB).
+    if (++g->material_uploads == 2 && !g->mirrors_pinned) {
+        cudaHostRegister(g->h.ep, (size_t)g->n * 3 * sizeof(float), cudaHostRegisterDefault);
+        cudaHostRegister(g->h.mu, (size_t)g->n * 3 * sizeof(float), cudaHostRegisterDefault);
+        cudaHostRegister(g->h.sig, (size_t)g->n * 6 * sizeof(float), cudaHostRegisterDefault);
+        cudaGetLastError();
+        g->mirrors_pinned = true;
+    }
     if (dirty & kMatEp) {
         CK(cudaMemsetAsync(g->d_flag + 0, 0, 3 * sizeof(int), g->st));
         if (!upload_deinterleave(g, g->h.ep, 3, g->ep, 1.0f, g->d_flag + 0)) return false;
@@ -546,11 +556,6 @@ bool grid_ensure_device(Grid *g)
         if (!dalloc(&g->d_jobs, g->jobs_cap * sizeof(OverlapJob), g->st, false)) return false;
         if (!dalloc(&g->d_partials, (size_t)g->jobs_cap * overlap_parts(g->nx, g->ny) * sizeof(double2), g->st, false))
             return false;
-        // pin the host mirrors the engine transfers (best effort)
-        cudaHostRegister(g->h.ep, (size_t)g->n * 3 * sizeof(float), cudaHostRegisterDefault);
-        cudaHostRegister(g->h.mu, (size_t)g->n * 3 * sizeof(float), cudaHostRegisterDefault);
-        cudaHostRegister(g->h.sig, (size_t)g->n * 6 * sizeof(float), cudaHostRegisterDefault);
-        cudaGetLastError();
         g->mat_dirty = kMatAll;
     }
     if (!g->f[0][0]) {

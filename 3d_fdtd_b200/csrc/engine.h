@@ -95,6 +95,8 @@ struct Grid {
     cudaStream_t side = nullptr;      // second stream of the flat4 CPML shell kernels
     unsigned *d_done = nullptr;       // completion count of the step-tail kernel
     bool in_run = false;              // steps enqueued by run_steps end with the step-tail kernel
+    int material_uploads = 0;         // the host mirrors are pinned at the second upload
+    bool mirrors_pinned = false;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     void *f[2][6] = {};       // field sets; set 1 is the ping-pong buffer of the fused path
     int cur = 0;

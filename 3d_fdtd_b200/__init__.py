@@ -158,6 +158,8 @@ SIGNATURES = {
     "fdtd_mode_solve_restarts": (i, []),
     "fdtd_mode_apply_beta_squared": (i, [Mode, d, Mode]),
     "fdtd_spline_basis": (i, [i, i, i, dp]),
+    "fdtd_gemm_bf16": (i, [C.c_void_p, i, C.c_void_p, i, i, i, i, C.c_void_p, i, C.c_float, C.c_float, C.c_void_p,
+                           i, C.c_void_p, i, C.c_void_p, i, C.c_void_p, C.c_void_p]),
     "timefield3d_set_spline_taper": (i, [T, d, d, i, dp, d, i, i, i, i]),
     "fdtd_spline_store_new": (C.c_void_p, [T, i, dp, d, i, i, i, i, i]),
     "fdtd_spline_store_bind": (i, [C.c_void_p, T, i, i, i]),

@@ -344,6 +344,17 @@ int fdtd_spline_store_unbind(fdtd_spline_store store, timefield3d psi);
 int fdtd_spline_store_gradient(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient);
 void fdtd_spline_store_free(fdtd_spline_store store);
 
+/* BF16 GEMM on the tcgen05 tensor cores (no reference counterpart; the
+ * surrogate network's contractions).  Device pointers, queued on `stream`:
+ *   pre = alpha A B^T + beta C32 + bias, Z32 = pre, post = act(pre) (0 identity,
+ *   1 GELU), C32 = post (FP32), C16 = post (BF16); any output may be NULL.
+ * A is M x K, B is N x K, both row-major with K contiguous (lda, ldb and K
+ * multiples of 8, operands 16-byte aligned); FP32 accumulation in tensor
+ * memory.  *err (device int) is set if a bounded internal wait gave up. */
+int fdtd_gemm_bf16(const void *A, int lda, const void *B, int ldb, int M, int N, int K, const float *bias, int act,
+                   float alpha, float beta, float *C32, int ldc32, void *C16, int ldc16, float *Z32, int ldz,
+                   int *err, void *stream);
+
 /* Self-test of the engine's bounded device waits (no reference counterpart):
  * one block waits, with the routine the TMA pipeline uses, on a barrier that
  * nothing arrives on.  Expected result FDTD_ERR_TIMEOUT after about

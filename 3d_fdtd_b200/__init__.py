@@ -158,6 +158,18 @@ SIGNATURES = {
     "fdtd_mode_solve_restarts": (i, []),
     "fdtd_mode_apply_beta_squared": (i, [Mode, d, Mode]),
     "fdtd_spline_basis": (i, [i, i, i, dp]),
+    "fdtd_mlp_new": (C.c_void_p, [i, i, i, C.c_ulonglong]),
+    "fdtd_mlp_param_count": (ll, [C.c_void_p]),
+    "fdtd_mlp_get_params": (i, [C.c_void_p, C.POINTER(C.c_float)]),
+    "fdtd_mlp_set_params": (i, [C.c_void_p, C.POINTER(C.c_float)]),
+    "fdtd_mlp_forward": (i, [C.c_void_p, C.POINTER(C.c_float), i, C.POINTER(C.c_float)]),
+    "fdtd_mlp_gradients": (i, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), i, C.POINTER(C.c_float),
+                               C.POINTER(C.c_double)]),
+    "fdtd_mlp_train_step": (i, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), i, C.c_float,
+                                C.POINTER(C.c_double)]),
+    "fdtd_mlp_input_gradient": (i, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), i,
+                                    C.POINTER(C.c_float)]),
+    "fdtd_mlp_free": (None, [C.c_void_p]),
     "fdtd_gemm_bf16": (i, [C.c_void_p, i, C.c_void_p, i, i, i, i, C.c_void_p, i, C.c_float, C.c_float, C.c_void_p,
                            i, C.c_void_p, i, C.c_void_p, i, C.c_void_p, C.c_void_p]),
     "timefield3d_set_spline_taper": (i, [T, d, d, i, dp, d, i, i, i, i]),

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include "common.cuh"
 
@@ -163,5 +164,24 @@ void launch_taper_store(const T *const *f_dev, const long long *cells, int ncell
 template <typename T>
 void launch_ep_gradient(const T *fwd, const T *adj, int ncell, int duration, double *grad, cudaStream_t st);
 void launch_check_finite(const float *a, long long n, int *bad, cudaStream_t st);
+
+// umma_gemm.cu: BF16 GEMM on tcgen05 (pre = alpha A B^T + beta C32 + bias;
+// act 0 identity / 1 GELU; A [M][lda], B [N][ldb], K-major)
+struct GemmArgs {
+    const __nv_bfloat16 *A;
+    const __nv_bfloat16 *B;
+    int lda, ldb, M, N, K;
+    const float *bias;
+    int act;
+    float alpha, beta;
+    float *C32;
+    int ldc32;
+    __nv_bfloat16 *C16;
+    int ldc16;
+    float *Z32;
+    int ldz;
+    int *err;
+};
+bool gemm_bf16_launch(const GemmArgs &a, cudaStream_t st);
 
 }  // namespace fdtd

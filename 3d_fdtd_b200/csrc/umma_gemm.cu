@@ -34,22 +34,6 @@ constexpr unsigned kGemmSBO = (kGemmBK / 8) * 128;   // bytes between 8-row grou
 constexpr unsigned kGemmLBO = 128;                   // bytes between the two K halves of a step
 constexpr unsigned long long kGemmWaitNs = 1000000000ull;
 
-struct GemmArgs {
-    const __nv_bfloat16 *A;
-    const __nv_bfloat16 *B;
-    int lda, ldb, M, N, K;
-    const float *bias;
-    int act;              // 0 identity, 1 GELU (erf form)
-    float alpha, beta;
-    float *C32;
-    int ldc32;
-    __nv_bfloat16 *C16;
-    int ldc16;
-    float *Z32;
-    int ldz;
-    int *err;
-};
-
 __device__ __forceinline__ unsigned su32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ unsigned long long gtime()

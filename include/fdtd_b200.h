@@ -355,6 +355,24 @@ int fdtd_gemm_bf16(const void *A, int lda, const void *B, int ldb, int M, int N,
                    float alpha, float beta, float *C32, int ldc32, void *C16, int ldc16, float *Z32, int ldz,
                    int *err, void *stream);
 
+/* Surrogate network of the taper optimiser (no reference counterpart): MLP
+ * n_in -> hidden x3 -> n_out, GELU, BF16 weights and activations with FP32
+ * accumulation on the tensor cores, FP32 master weights and Adam.  Host
+ * arrays, row-major [batch][n]; batch a multiple of 8.  Parameters in flat
+ * order W1 [hidden][n_in], b1, W2, b2, W3, b3, W4 [n_out][hidden], b4. */
+void *fdtd_mlp_new(int n_in, int hidden, int n_out, unsigned long long seed);
+long long fdtd_mlp_param_count(void *net);
+int fdtd_mlp_get_params(void *net, float *params);
+int fdtd_mlp_set_params(void *net, const float *params);   /* also resets Adam */
+int fdtd_mlp_forward(void *net, const float *x, int batch, float *y);
+/* gradients of the mean squared error (no update) */
+int fdtd_mlp_gradients(void *net, const float *x, const float *target, int batch, float *grad, double *loss);
+/* forward, backward and one Adam step (beta 0.9 / 0.999, eps 1e-8) */
+int fdtd_mlp_train_step(void *net, const float *x, const float *target, int batch, float lr, double *loss);
+/* dx = (dy/dx)^T dy for each row */
+int fdtd_mlp_input_gradient(void *net, const float *x, const float *dy, int batch, float *dx);
+void fdtd_mlp_free(void *net);
+
 /* Self-test of the engine's bounded device waits (no reference counterpart):
  * one block waits, with the routine the TMA pipeline uses, on a barrier that
  * nothing arrives on.  Expected result FDTD_ERR_TIMEOUT after about

@@ -133,15 +133,19 @@ class Slot:
         self.fd.lib.timefield3d_zero_fields(self.grid.t)
         self.fd.call("timefield3d_run", self.grid.t, self.dt, self.T)
 
-    def transmission(self) -> np.ndarray:
-        """Waits for this slot's run; T(lambda) = |O_out / O_in|^2."""
+    def amplitudes(self) -> np.ndarray:
+        """Waits for this slot's run; complex t(lambda) = O_out / O_in."""
         fd, n = self.fd, len(self.omega)
         a, b = (fd.Complex * n)(), (fd.Complex * n)()
         fd.call("timefield3d_read_overlap_monitor", self.grid.t, self.mon_in, a)
         fd.call("timefield3d_read_overlap_monitor", self.grid.t, self.mon_out, b)
         oi = np.array([complex(x.re, x.im) for x in a])
         oo = np.array([complex(x.re, x.im) for x in b])
-        return np.abs(oo / oi) ** 2
+        return oo / oi
+
+    def transmission(self) -> np.ndarray:
+        """Waits for this slot's run; T(lambda) = |O_out / O_in|^2."""
+        return np.abs(self.amplitudes()) ** 2
 
     def close(self):
         if self.grid is not None:
@@ -177,7 +181,7 @@ def sweep(fd, cands: list[dict], slots: int = 4, variant: int | None = None, ret
     Finished grids are kept (not freed) until about `retire_gb` of device
     memory is held by them, then freed together."""
     if not cands:
-        return dict(results={}, seconds=0.0, cell_steps=0, bytes=0, variant=variant, tuning={})
+        return dict(results={}, amplitudes={}, seconds=0.0, cell_steps=0, bytes=0, variant=variant, tuning={})
     tuning = {}
     if variant is None:
         variant, tuning = autotune(fd, cands[0])
@@ -195,6 +199,7 @@ def sweep(fd, cands: list[dict], slots: int = 4, variant: int | None = None, ret
             retired.clear()
 
     results = {}
+    amplitudes = {}
     cell_steps = 0
     nbytes = 0
     t0 = time.perf_counter()
@@ -207,7 +212,9 @@ def sweep(fd, cands: list[dict], slots: int = 4, variant: int | None = None, ret
     while busy:
         slot = busy.pop(0)
         c = slot.cand
-        results[c["index"]] = slot.transmission().tolist()
+        t = slot.amplitudes()
+        amplitudes[c["index"]] = t
+        results[c["index"]] = (np.abs(t) ** 2).tolist()
         nx, ny, nz = slot.shape
         cell_steps += nx * ny * nz * c["steps"]
         nbytes += algorithmic_bytes(nx, ny, nz, SPEC["cpml"]) * c["steps"]
@@ -220,8 +227,8 @@ def sweep(fd, cands: list[dict], slots: int = 4, variant: int | None = None, ret
         slot.close()
     for g in retired:
         g.close()
-    return dict(results=results, seconds=seconds, cell_steps=cell_steps, bytes=nbytes, variant=variant,
-                tuning={int(k): v for k, v in tuning.items()})
+    return dict(results=results, amplitudes=amplitudes, seconds=seconds, cell_steps=cell_steps, bytes=nbytes,
+                variant=variant, tuning={int(k): v for k, v in tuning.items()})
 
 
 def main():

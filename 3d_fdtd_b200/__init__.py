@@ -158,6 +158,9 @@ SIGNATURES = {
     "fdtd_mode_solve_restarts": (i, []),
     "fdtd_mode_apply_beta_squared": (i, [Mode, d, Mode]),
     "fdtd_spline_basis": (i, [i, i, i, dp]),
+    "timefield3d_checkpoint_save": (i, [T, C.c_char_p]),
+    "timefield3d_checkpoint_load": (i, [T, C.c_char_p]),
+    "fdtd_inject_allocation_failures": (None, [i]),
     "fdtd_mlp_new": (C.c_void_p, [i, i, i, C.c_ulonglong]),
     "fdtd_mlp_param_count": (ll, [C.c_void_p]),
     "fdtd_mlp_get_params": (i, [C.c_void_p, C.POINTER(C.c_float)]),

@@ -1165,6 +1165,7 @@ int adjoint3d_taper_unbind_store(adjoint3d_taper taper, timefield3d psi)
 int timefield3d_run(timefield3d psi, double delta_t, int nsteps)
 {
     LOCK;
+    TraceRange tr("timefield3d_run");
     Grid *g = dev_grid(psi);
     if (!g) return fdtd_last_error();
     if (nsteps < 0) {
@@ -1289,9 +1290,36 @@ void *timefield3d_get_stream(timefield3d psi)
 int timefield3d_upload_materials(timefield3d psi)
 {
     LOCK;
+    TraceRange tr("timefield3d_upload_materials");
     Grid *g = dev_grid(psi);
     if (!g) return fdtd_last_error();
     return grid_upload_materials(g) ? FDTD_OK : fdtd_last_error();
+}
+
+int timefield3d_checkpoint_save(timefield3d psi, const char *path)
+{
+    LOCK;
+    TraceRange tr("timefield3d_checkpoint_save");
+    Grid *g = dev_grid(psi);
+    if (!g) return fdtd_last_error();
+    if (!path) return FDTD_ERR_ARG;
+    return grid_checkpoint_save(g, path) ? FDTD_OK : fdtd_last_error();
+}
+
+int timefield3d_checkpoint_load(timefield3d psi, const char *path)
+{
+    LOCK;
+    TraceRange tr("timefield3d_checkpoint_load");
+    Grid *g = dev_grid(psi);
+    if (!g) return fdtd_last_error();
+    if (!path) return FDTD_ERR_ARG;
+    return grid_checkpoint_load(g, path) ? FDTD_OK : fdtd_last_error();
+}
+
+void fdtd_inject_allocation_failures(int n)
+{
+    LOCK;
+    inject_allocation_failures(n);
 }
 
 int timefield3d_set_kernel_timing(timefield3d psi, int on)

@@ -2,6 +2,8 @@
 // CUDA-graph capture of multi-step runs.
 #include "engine.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -85,9 +87,21 @@ std::mutex &api_mutex()
     return m;
 }
 
+TraceRange::TraceRange(const char *name) { nvtxRangePushA(name); }
+TraceRange::~TraceRange() { nvtxRangePop(); }
+
+// host-side fault injection: the next n engine allocations report failure
+static std::atomic<int> g_fail_allocs{0};
+void inject_allocation_failures(int n) { g_fail_allocs.store(n < 0 ? 0 : n); }
+
 template <typename P> static bool dalloc(P **p, size_t bytes, cudaStream_t st, bool zero = true)
 {
     if (*p) return true;
+    if (g_fail_allocs.load() > 0) {
+        g_fail_allocs--;
+        set_error(FDTD_ERR_ALLOC, "device allocation of %zu bytes failed (injected)", bytes);
+        return false;
+    }
     void *v = nullptr;
     if (!cuda_ok(cudaMalloc(&v, bytes ? bytes : 16), "cudaMalloc")) return false;
     *p = (P *)v;
@@ -1250,6 +1264,159 @@ bool enqueue_taper_store(TaperDev *td, Grid *g, int which, int t_index, const lo
         launch_taper_store<float>((const float *const *)fp, td->d_cells, td->ncell, (float *)store, t_index, d_step, t0, dir, td->duration, g->st);
     CKL("taper store");
     return true;
+}
+
+// ============================================================================
+// checkpoint / resume
+// ============================================================================
+// File: "FDTDCKP1", int32 nx ny nz precision boundary L n_monitors n_planes
+// has_psi, int64 host_steps device_step, per monitor int32 nfreq + 2 nfreq
+// double2, per plane int32 k + 6 nx ny float, the 6 field components of the
+// current set (n elements of the grid's precision), then (has_psi) the 12
+// CPML auxiliary arrays of the current set.  Materials, modes, schedules and
+// monitor definitions are the caller's set-up and are not stored.
+namespace {
+struct FileCloser {
+    FILE *f;
+    ~FileCloser() { if (f) fclose(f); }
+};
+bool wr(FILE *f, const void *p, size_t n) { return fwrite(p, 1, n, f) == n; }
+bool rd(FILE *f, void *p, size_t n) { return fread(p, 1, n, f) == n; }
+}  // namespace
+
+static void psi_sizes(const Grid *g, size_t sz[3])
+{
+    const size_t L2 = 2 * (size_t)g->L, es = esize(g);
+    sz[0] = L2 * g->ny * g->nz * es;
+    sz[1] = (size_t)g->nx * L2 * g->nz * es;
+    sz[2] = (size_t)g->nx * g->ny * L2 * es;
+}
+
+bool grid_checkpoint_save(Grid *g, const char *path)
+{
+    if (!grid_ensure_device(g)) return false;
+    CK(cudaStreamSynchronize(g->st));
+    FileCloser fc{fopen(path, "wb")};
+    if (!fc.f) {
+        set_error(FDTD_ERR_ARG, "checkpoint: cannot open %s for writing", path);
+        return false;
+    }
+    const bool has_psi = g->boundary == FDTD_BOUNDARY_CPML && g->psi[g->cur][0][0];
+    int hdr[9] = {g->nx, g->ny, g->nz, g->prec, g->boundary, g->L, (int)g->monitors.size(), (int)g->planes.size(),
+                  has_psi ? 1 : 0};
+    long long dstep = 0;
+    CK(cudaMemcpy(&dstep, g->d_step, sizeof(long long), cudaMemcpyDeviceToHost));
+    long long steps[2] = {g->host_steps, dstep};
+    bool ok = wr(fc.f, "FDTDCKP1", 8) && wr(fc.f, hdr, sizeof hdr) && wr(fc.f, steps, sizeof steps);
+    std::vector<char> buf;
+    for (auto &mn : g->monitors) {
+        buf.resize(2 * (size_t)mn.nfreq * sizeof(double2));
+        CK(cudaMemcpy(buf.data(), mn.d_acc, buf.size(), cudaMemcpyDeviceToHost));
+        ok = ok && wr(fc.f, &mn.nfreq, sizeof(int)) && wr(fc.f, buf.data(), buf.size());
+    }
+    const size_t pb = 6 * (size_t)g->nx * g->ny * sizeof(float);
+    for (auto &pl : g->planes) {
+        buf.resize(pb);
+        CK(cudaMemcpy(buf.data(), pl.p, pb, cudaMemcpyDeviceToHost));
+        ok = ok && wr(fc.f, &pl.k, sizeof(int)) && wr(fc.f, buf.data(), pb);
+    }
+    const size_t fb = (size_t)g->n * esize(g);
+    buf.resize(fb);
+    for (int m = 0; m < 6 && ok; m++) {
+        CK(cudaMemcpy(buf.data(), g->f[g->cur][m], fb, cudaMemcpyDeviceToHost));
+        ok = wr(fc.f, buf.data(), fb);
+    }
+    if (has_psi) {
+        size_t sz[3];
+        psi_sizes(g, sz);
+        for (int a = 0; a < 3; a++)
+            for (int w = 0; w < 4 && ok; w++) {
+                buf.resize(sz[a]);
+                CK(cudaMemcpy(buf.data(), g->psi[g->cur][a][w], sz[a], cudaMemcpyDeviceToHost));
+                ok = wr(fc.f, buf.data(), sz[a]);
+            }
+    }
+    if (!ok) {
+        set_error(FDTD_ERR_ALLOC, "checkpoint: short write to %s", path);
+        return false;
+    }
+    return true;
+}
+
+bool grid_checkpoint_load(Grid *g, const char *path)
+{
+    if (!grid_ensure_device(g)) return false;
+    CK(cudaStreamSynchronize(g->st));
+    FileCloser fc{fopen(path, "rb")};
+    if (!fc.f) {
+        set_error(FDTD_ERR_ARG, "checkpoint: cannot open %s", path);
+        return false;
+    }
+    char magic[8];
+    int hdr[9];
+    long long steps[2];
+    if (!rd(fc.f, magic, 8) || memcmp(magic, "FDTDCKP1", 8) != 0 || !rd(fc.f, hdr, sizeof hdr) ||
+        !rd(fc.f, steps, sizeof steps)) {
+        set_error(FDTD_ERR_ARG, "checkpoint: %s is not a checkpoint of this library", path);
+        return false;
+    }
+    if (hdr[0] != g->nx || hdr[1] != g->ny || hdr[2] != g->nz || hdr[3] != g->prec || hdr[4] != g->boundary ||
+        (g->boundary == FDTD_BOUNDARY_CPML && hdr[5] != g->L) || hdr[6] != (int)g->monitors.size()) {
+        set_error(FDTD_ERR_ARG,
+                  "checkpoint: saved grid %dx%dx%d precision %d boundary %d L %d with %d monitors does not match this "
+                  "grid (%dx%dx%d precision %d boundary %d L %d, %d monitors)",
+                  hdr[0], hdr[1], hdr[2], hdr[3], hdr[4], hdr[5], hdr[6], g->nx, g->ny, g->nz, g->prec, g->boundary,
+                  g->L, (int)g->monitors.size());
+        return false;
+    }
+    std::vector<char> buf;
+    for (auto &mn : g->monitors) {
+        int nf = 0;
+        if (!rd(fc.f, &nf, sizeof nf) || nf != mn.nfreq) {
+            set_error(FDTD_ERR_ARG, "checkpoint: monitor frequency count %d does not match %d", nf, mn.nfreq);
+            return false;
+        }
+        buf.resize(2 * (size_t)nf * sizeof(double2));
+        if (!rd(fc.f, buf.data(), buf.size())) goto short_read;
+        CK(cudaMemcpy(mn.d_acc, buf.data(), buf.size(), cudaMemcpyHostToDevice));
+    }
+    {
+        const size_t pb = 6 * (size_t)g->nx * g->ny * sizeof(float);
+        for (int q = 0; q < hdr[7]; q++) {
+            int k = 0;
+            buf.resize(pb);
+            if (!rd(fc.f, &k, sizeof k) || !rd(fc.f, buf.data(), pb)) goto short_read;
+            Plane *pl = grid_plane(g, k, true);
+            if (!pl) return false;
+            CK(cudaMemcpy(pl->p, buf.data(), pb, cudaMemcpyHostToDevice));
+        }
+        const size_t fb = (size_t)g->n * esize(g);
+        buf.resize(fb);
+        for (int m = 0; m < 6; m++) {
+            if (!rd(fc.f, buf.data(), fb)) goto short_read;
+            CK(cudaMemcpy(g->f[g->cur][m], buf.data(), fb, cudaMemcpyHostToDevice));
+        }
+        if (hdr[8]) {
+            size_t sz[3];
+            psi_sizes(g, sz);
+            for (int a = 0; a < 3; a++)
+                for (int w = 0; w < 4; w++) {
+                    buf.resize(sz[a]);
+                    if (!rd(fc.f, buf.data(), sz[a])) goto short_read;
+                    if (!dalloc(&g->psi[g->cur][a][w], sz[a], g->st)) return false;
+                    CK(cudaMemcpy(g->psi[g->cur][a][w], buf.data(), sz[a], cudaMemcpyHostToDevice));
+                }
+        }
+    }
+    CK(cudaMemcpy(g->d_step, &steps[1], sizeof(long long), cudaMemcpyHostToDevice));
+    g->host_steps = steps[0];
+    g->fields_from_host = false;
+    g->pp_synced = false;
+    g->version++;
+    return true;
+short_read:
+    set_error(FDTD_ERR_ARG, "checkpoint: %s is truncated", path);
+    return false;
 }
 
 }  // namespace fdtd

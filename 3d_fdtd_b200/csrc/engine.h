@@ -195,6 +195,16 @@ bool grid_set_precision(Grid *g, int prec);
 bool grid_prepare_step(Grid *g, double dt);    // profiles / coefficients for dt
 Plane *grid_plane(Grid *g, int k, bool create);
 void grid_zero(Grid *g);
+bool grid_checkpoint_save(Grid *g, const char *path);
+bool grid_checkpoint_load(Grid *g, const char *path);
+void inject_allocation_failures(int n);
+
+// NVTX range for the duration of a scope (tracing with nsys / ncu; a no-op
+// without a tool attached)
+struct TraceRange {
+    explicit TraceRange(const char *name);
+    ~TraceRange();
+};
 
 // queued work
 bool enqueue_step(Grid *g, double dt, bool with_extras);

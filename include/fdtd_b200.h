@@ -373,6 +373,19 @@ int fdtd_mlp_train_step(void *net, const float *x, const float *target, int batc
 int fdtd_mlp_input_gradient(void *net, const float *x, const float *dy, int batch, float *dx);
 void fdtd_mlp_free(void *net);
 
+/* Checkpoint / resume (no reference counterpart): the current fields, CPML
+ * auxiliaries, step counters, overlap-monitor accumulators and source planes
+ * of a grid, in one file.  Loading needs a grid of the same size, precision,
+ * boundary (CPML thickness) and number of monitors with the same frequency
+ * counts, set up by the caller as before (materials, modes, schedules);
+ * continuing from a loaded checkpoint gives the same results, bit for bit, as
+ * never stopping.  Taper edge stores are not included. */
+int timefield3d_checkpoint_save(timefield3d psi, const char *path);
+int timefield3d_checkpoint_load(timefield3d psi, const char *path);
+/* Host-side fault injection for tests: the next n device allocations of the
+ * grid engine report FDTD_ERR_ALLOC without touching the GPU (0 clears). */
+void fdtd_inject_allocation_failures(int n);
+
 /* Self-test of the engine's bounded device waits (no reference counterpart):
  * one block waits, with the routine the TMA pipeline uses, on a barrier that
  * nothing arrives on.  Expected result FDTD_ERR_TIMEOUT after about

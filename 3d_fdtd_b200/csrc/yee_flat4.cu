@@ -435,7 +435,8 @@ __global__ void __launch_bounds__(kBlock4, W == 4 ? (SLABS ? 2 : 4) : 3) k_flat4
 {
     int g, j, k;
     bool live;
-    locate<KIND>(r, a.nx / W, a.ny, blockIdx.x * kBlock4 + threadIdx.x, blockIdx.y, g, j, k, live);
+    // planes in descending order: see k_flat4_merged
+    locate<KIND>(r, a.nx / W, a.ny, blockIdx.x * kBlock4 + threadIdx.x, gridDim.y - 1 - blockIdx.y, g, j, k, live);
     h_cells<W, SLABS>(a, g, j, k, live);
 }
 
@@ -444,10 +445,14 @@ __global__ void __launch_bounds__(kBlock4, W == 4 ? (SLABS ? 2 : 4) : 3) k_flat4
 //   planes 1..L-1, nz-L..nz-2: nbz blocks of the z-slab region (W 2, SLABS 7)
 //   planes L..nz-L-1: nb_box box blocks (W 4, plain), nb_y y-slab-row blocks
 //   (W 2, SLABS 2), nb_x x-slab-column blocks (W 2, SLABS 3)
+// The E launch walks the planes upwards and the H launch downwards: the E
+// planes the H launch reads first are the ones the E launch wrote last (still
+// in the 126 MB L2), and the H planes the next E launch reads first are the
+// ones the H launch wrote last.  Block order does not change any result.
 template <bool E_FIELD, bool LOSSY>
 __global__ void __launch_bounds__(kBlock4, E_FIELD ? 3 : 4) k_flat4_merged(FlatArgs a, Plan4 p)
 {
-    int b = blockIdx.x;
+    int b = E_FIELD ? (int)blockIdx.x : (int)(gridDim.x - 1 - blockIdx.x);
     const int nzs = (p.L - 1) * p.nbz, nmb = p.nmid * p.nbm;
     int plane, lb;
     bool zslab;

@@ -452,6 +452,12 @@ __global__ void __launch_bounds__(kBlock4, W == 4 ? (SLABS ? 2 : 4) : 3) k_flat4
 template <bool E_FIELD, bool LOSSY>
 __global__ void __launch_bounds__(kBlock4, E_FIELD ? 3 : 4) k_flat4_merged(FlatArgs a, Plan4 p)
 {
+    // Programmatic dependent launch: every E block lets the H launch start
+    // scheduling (its blocks then fill SMs freed by the E tail); the H blocks
+    // wait here until the E grid has completed and its stores are visible.
+    // Both are no-ops in a launch without the attribute.
+    if (E_FIELD) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    else asm volatile("griddepcontrol.wait;" ::: "memory");
     int b = E_FIELD ? (int)blockIdx.x : (int)(gridDim.x - 1 - blockIdx.x);
     const int nzs = (p.L - 1) * p.nbz, nmb = p.nmid * p.nbm;
     int plane, lb;
@@ -588,12 +594,22 @@ void launch_flat4_step(const FlatArgs &a, cudaStream_t st, cudaStream_t side, cu
     const long long blocks = 2LL * (L - 1) * p.nbz + (long long)nmid * p.nbm;
     const bool lossy = a.ca[0] != nullptr;
     note_launch(2);
+    // H launch with a programmatic dependency on the E launch (see k_flat4_merged)
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3(kBlock4);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     if (lossy) {
         k_flat4_merged<true, true><<<(unsigned)blocks, kBlock4, 0, st>>>(a, p);
-        k_flat4_merged<false, true><<<(unsigned)blocks, kBlock4, 0, st>>>(a, p);
+        cudaLaunchKernelEx(&cfg, k_flat4_merged<false, true>, a, p);
     } else {
         k_flat4_merged<true, false><<<(unsigned)blocks, kBlock4, 0, st>>>(a, p);
-        k_flat4_merged<false, false><<<(unsigned)blocks, kBlock4, 0, st>>>(a, p);
+        cudaLaunchKernelEx(&cfg, k_flat4_merged<false, false>, a, p);
     }
     (void)side; (void)fork; (void)join;
 }

@@ -30,7 +30,7 @@ __device__ __forceinline__ void schedule_values(const SourceJob &sj, long long n
     }
 }
 
-// cells t = first, first + stride, ... of the source plane
+// window cells u = first, first + stride, ... of the source plane
 __device__ __forceinline__ void mode_source_cells(const SourceJob &sj, long long first, long long stride, double A,
                                                   double c, double s)
 {
@@ -38,8 +38,10 @@ __device__ __forceinline__ void mode_source_cells(const SourceJob &sj, long long
     const long long nxy = (long long)nx * sj.ny;
     const int M_sign = -1 + 2 * sj.reverse;
     float *plane = sj.plane;
-    for (long long t = first; t < nxy; t += stride) {
-        int i = (int)(t % nx), j = (int)(t / nx);
+    const long long cells = (long long)sj.win.wni * sj.win.wnj;
+    for (long long u = first; u < cells; u += stride) {
+        const int i = sj.win.wi + (int)(u % sj.win.wni), j = sj.win.wj + (int)(u / sj.win.wni);
+        const long long t = i + (long long)nx * j;
         double xd = dmul((double)(i - sj.cx), sj.ratio);
         double yd = dmul((double)(j - sj.cy), sj.ratio);
         int mx = (int)xd + sj.mi / 2, my = (int)yd + sj.mj / 2;
@@ -94,9 +96,11 @@ __device__ __forceinline__ void overlap_block(const T *const *Ex_, int nx, int n
     const long long nxy = (long long)nx * ny;
     const T *Ex = Ex_[0], *Ey = Ex_[1], *Hx = Ex_[3], *Hy = Ex_[4];
     const long long base = nxy * jb.cz;
+    const long long cells = (long long)jb.win.wni * jb.win.wnj;
     double sre = 0.0, sim = 0.0;
-    for (long long t = part * (long long)blockDim.x + threadIdx.x; t < nxy; t += (long long)nparts * blockDim.x) {
-        int i = (int)(t % nx), j = (int)(t / nx);
+    for (long long u = part * (long long)blockDim.x + threadIdx.x; u < cells; u += (long long)nparts * blockDim.x) {
+        const int i = jb.win.wi + (int)(u % jb.win.wni), j = jb.win.wj + (int)(u / jb.win.wni);
+        const long long t = i + (long long)nx * j;
         double xd = dmul((double)(i - jb.cx), jb.ratio);
         double yd = dmul((double)(j - jb.cy), jb.ratio);
         int mx = (int)xd + jb.mi / 2, my = (int)yd + jb.mj / 2;
@@ -215,6 +219,12 @@ constexpr int kTailJobs = 64;
 template <typename T>
 __global__ void __launch_bounds__(256) k_step_tail(TailArgs a)
 {
+    // Programmatic dependent launch (no-ops in a plain launch): wait until the
+    // H update has completed and its stores are visible -- that also orders the
+    // source plane write after the E update that read it -- then let the next
+    // step's E update start scheduling; its blocks wait for this grid in turn.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int nov = a.njobs * a.nparts;
     const int b = blockIdx.x;
     if (b < nov) {
@@ -258,11 +268,13 @@ __global__ void __launch_bounds__(256) k_step_tail(TailArgs a)
             if (jb.inst) *jb.inst = tot[jid];
         }
         __syncthreads();
-        // one thread per (job, frequency)
-        for (int jid = 0; jid < a.njobs; jid++) {
+        // one warp per job, one lane per frequency: the jobs' loads, phases
+        // and stores overlap instead of following one another
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for (int jid = warp; jid < a.njobs; jid += blockDim.x >> 5) {
             const OverlapJob jb = a.jobs[jid];
             if (!jb.acc) continue;
-            for (int f = threadIdx.x; f < jb.nfreq; f += blockDim.x) accumulate_frequency(jb, f, tot[jid], a.dt, n);
+            for (int f = lane; f < jb.nfreq; f += 32) accumulate_frequency(jb, f, tot[jid], a.dt, n);
         }
     } else {
         for (int jid = 0; jid < a.njobs; jid++) {
@@ -370,11 +382,11 @@ __global__ void k_check_finite(const float *a, long long n, int *bad)
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
-static int source_blocks(int nx, int ny)
+static int source_blocks(const ModeWindow &w)
 {
-    long long nxy = (long long)nx * ny;
-    int blocks = (int)((nxy + 255) / 256);
-    return blocks > 1184 ? 1184 : blocks;
+    const long long cells = (long long)w.wni * w.wnj;
+    const long long blocks = (cells + 255) / 256;
+    return blocks < 1 ? 1 : blocks > 1184 ? 1184 : (int)blocks;
 }
 
 void launch_mode_source(float *plane, const float *const ep_plane[3], const float *const mu_plane[3], int nx, int ny,
@@ -391,25 +403,42 @@ void launch_mode_source(float *plane, const float *const ep_plane[3], const floa
     launch_mode_source_job(sj, amplitude, cph, sph, step, 0, st);
 }
 
-void launch_mode_source_job(const SourceJob &sj, double amplitude, double cph, double sph, const long long *step,
+void launch_mode_source_job(const SourceJob &sj_in, double amplitude, double cph, double sph, const long long *step,
                             int step_offset, cudaStream_t st)
 {
+    SourceJob sj = sj_in;
+    sj.win = mode_window(sj.nx, sj.ny, sj.cx, sj.cy, sj.mi, sj.mj, sj.ratio);
     note_launch();
-    k_mode_source<<<source_blocks(sj.nx, sj.ny), 256, 0, st>>>(sj, amplitude, cph, sph, step, step_offset);
+    k_mode_source<<<source_blocks(sj.win), 256, 0, st>>>(sj, amplitude, cph, sph, step, step_offset);
 }
 
 template <typename T>
 void launch_step_tail(TailArgs a, cudaStream_t st)
 {
-    a.nparts = overlap_parts(a.nx, a.ny);
-    a.src_blocks = a.src.plane ? source_blocks(a.src.nx, a.src.ny) : 0;
+    a.nparts = a.njobs > 0 ? overlap_parts(a.cells) : 0;
+    if (a.src.plane) {
+        a.src.win = mode_window(a.src.nx, a.src.ny, a.src.cx, a.src.cy, a.src.mi, a.src.mj, a.src.ratio);
+        a.src_blocks = source_blocks(a.src.win);
+    } else {
+        a.src_blocks = 0;
+    }
     const int blocks = a.njobs * a.nparts + a.src_blocks;
     note_launch();
     if (blocks == 0) {
         k_step_advance<<<1, 1, 0, st>>>(a.step);
         return;
     }
-    k_step_tail<T><<<blocks, 256, 0, st>>>(a);
+    // launched with a programmatic dependency on the preceding kernel (see k_step_tail)
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_step_tail<T>, a);
 }
 template void launch_step_tail<float>(TailArgs, cudaStream_t);
 template void launch_step_tail<double>(TailArgs, cudaStream_t);
@@ -420,19 +449,20 @@ void launch_set_value(float *p, long long idx, float v, cudaStream_t st)
     k_set_value<<<1, 1, 0, st>>>(p, idx, v);
 }
 
-int overlap_parts(int nx, int ny)
+// partials per overlap job: one 256-thread block per 256 window cells, 1 to 64
+int overlap_parts(long long cells)
 {
-    long long nxy = (long long)nx * ny;
-    long long b = (nxy + 255) / 256;
-    return (int)(b < 64 ? b : 64);
+    const long long b = (cells + 255) / 256;
+    return (int)(b < 1 ? 1 : b > 64 ? 64 : b);
 }
 
 template <typename T>
-void launch_overlap(const T *const *f_dev, int nx, int ny, const OverlapJob *jobs_dev, int njobs, double2 *partials,
-                    double scale, double dt, const long long *step, int step_offset, cudaStream_t st)
+void launch_overlap(const T *const *f_dev, int nx, int ny, const OverlapJob *jobs_dev, int njobs, long long cells,
+                    double2 *partials, double scale, double dt, const long long *step, int step_offset,
+                    cudaStream_t st)
 {
     if (njobs <= 0) return;
-    int parts = overlap_parts(nx, ny);
+    const int parts = overlap_parts(cells);
     note_launch();
     k_overlap_partial<T><<<dim3(parts, njobs), 256, 0, st>>>(f_dev, nx, ny, jobs_dev, partials, parts);
     note_launch();
@@ -496,8 +526,8 @@ void launch_check_finite(const float *a, long long n, int *bad, cudaStream_t st)
 }
 
 #define FDTD_INST(T)                                                                                               \
-    template void launch_overlap<T>(const T *const *, int, int, const OverlapJob *, int, double2 *, double, double, \
-                                    const long long *, int, cudaStream_t);                                         \
+    template void launch_overlap<T>(const T *const *, int, int, const OverlapJob *, int, long long, double2 *,     \
+                                    double, double, const long long *, int, cudaStream_t);                         \
     template void launch_dft<T>(const T *const *, int, int, int, int, int, int, double, double, double2 *,         \
                                 cudaStream_t);                                                                     \
     template void launch_probes<T>(const T *const *, const ProbeJob *, int, double *, int, int *, cudaStream_t);   \

@@ -599,12 +599,16 @@ complex timefield3d_mode_overlap(timefield3d psi, int center_x, int center_y, in
     j.acc = nullptr;
     j.omega = nullptr;
     j.nfreq = 0;
+    j.win = mode_window(g->nx, g->ny, j.cx, j.cy, j.mi, j.mj, j.ratio);
     if (!cuda_ok(cudaMemcpyAsync(g->d_job1, &j, sizeof j, cudaMemcpyHostToDevice, g->st), "overlap job")) return inst;
     const double scale = (-0.5 * psi.disc * psi.disc);
+    const long long cells = (long long)j.win.wni * j.win.wnj;
     if (g->prec == FDTD_F64)
-        launch_overlap<double>((const double *const *)fptr(g), g->nx, g->ny, g->d_job1, 1, g->d_partials, scale, 0, g->d_step, 0, g->st);
+        launch_overlap<double>((const double *const *)fptr(g), g->nx, g->ny, g->d_job1, 1, cells, g->d_partials, scale,
+                               0, g->d_step, 0, g->st);
     else
-        launch_overlap<float>((const float *const *)fptr(g), g->nx, g->ny, g->d_job1, 1, g->d_partials, scale, 0, g->d_step, 0, g->st);
+        launch_overlap<float>((const float *const *)fptr(g), g->nx, g->ny, g->d_job1, 1, cells, g->d_partials, scale,
+                              0, g->d_step, 0, g->st);
     if (!cuda_ok(cudaMemcpyAsync(g->h_inst, g->d_inst, sizeof(double2), cudaMemcpyDeviceToHost, g->st), "overlap D2H") ||
         !cuda_ok(cudaStreamSynchronize(g->st), "overlap sync"))
         return inst;
@@ -1014,14 +1018,14 @@ int timefield3d_add_overlap_monitor(timefield3d psi, int center_x, int center_y,
         cudaFree(g->d_jobs); cudaFree(g->d_partials);
         g->d_jobs = nullptr; g->d_partials = nullptr;
         g->jobs_cap = (int)g->monitors.size() * 2;
-        int parts = overlap_parts(g->nx, g->ny);
+        int parts = overlap_parts((long long)g->nx * g->ny);
         if (!cuda_ok(cudaMalloc(&g->d_jobs, g->jobs_cap * sizeof(OverlapJob)), "cudaMalloc(jobs)") ||
             !cuda_ok(cudaMalloc(&g->d_partials, (size_t)g->jobs_cap * parts * sizeof(double2)), "cudaMalloc(partials)"))
             return -1;
     }
     if (!g->d_jobs) {
         g->jobs_cap = std::max(g->jobs_cap, 8);
-        int parts = overlap_parts(g->nx, g->ny);
+        int parts = overlap_parts((long long)g->nx * g->ny);
         if (!cuda_ok(cudaMalloc(&g->d_jobs, g->jobs_cap * sizeof(OverlapJob)), "cudaMalloc(jobs)") ||
             !cuda_ok(cudaMalloc(&g->d_partials, (size_t)g->jobs_cap * parts * sizeof(double2)), "cudaMalloc(partials)"))
             return -1;
@@ -1326,9 +1330,10 @@ int timefield3d_set_kernel_timing(timefield3d psi, int on)
 {
     LOCK;
     Grid *g = grid_lookup(psi);
-    if (!g) return FDTD_ERR_ARG;
+    if (!g || on < 0) return FDTD_ERR_ARG;
     if (g->dev && (!drain_kernel_timing(g, 0) || !drain_kernel_timing(g, 1))) return fdtd_last_error();
-    g->ktime = on != 0;
+    g->ktime = on;
+    g->kreplay = 0;
     g->ktime_ms = 0;
     g->ktime_n = 0;
     return FDTD_OK;

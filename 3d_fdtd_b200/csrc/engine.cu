@@ -568,8 +568,8 @@ bool grid_ensure_device(Grid *g)
         if (!dalloc(&g->d_job1, sizeof(OverlapJob), g->st)) return false;
         g->jobs_cap = 8;
         if (!dalloc(&g->d_jobs, g->jobs_cap * sizeof(OverlapJob), g->st, false)) return false;
-        if (!dalloc(&g->d_partials, (size_t)g->jobs_cap * overlap_parts(g->nx, g->ny) * sizeof(double2), g->st, false))
-            return false;
+        const int parts = overlap_parts((long long)g->nx * g->ny);
+        if (!dalloc(&g->d_partials, (size_t)g->jobs_cap * parts * sizeof(double2), g->st, false)) return false;
         g->mat_dirty = kMatAll;
     }
     if (!g->f[0][0]) {
@@ -773,7 +773,7 @@ bool grid_prepare_step(Grid *g, double dt)
         }
     }
     // overlap scratch for the monitors
-    int parts = overlap_parts(g->nx, g->ny);
+    int parts = overlap_parts((long long)g->nx * g->ny);
     int need = std::max<int>(1, (int)g->monitors.size());
     if (g->jobs_cap < need) {
         dfree(g->d_jobs);
@@ -917,8 +917,12 @@ bool enqueue_after_step(Grid *g, double dt)
     }
     const double scale = (-0.5 * g->dx * g->dx);
     if (g->njobs > 0 && !g->in_run) {
-        if (f64) launch_overlap<double>((const double *const *)fp, g->nx, g->ny, g->d_jobs, g->njobs, g->d_partials, scale, dt, g->d_step, 0, g->st);
-        else launch_overlap<float>((const float *const *)fp, g->nx, g->ny, g->d_jobs, g->njobs, g->d_partials, scale, dt, g->d_step, 0, g->st);
+        if (f64)
+            launch_overlap<double>((const double *const *)fp, g->nx, g->ny, g->d_jobs, g->njobs, g->job_cells,
+                                   g->d_partials, scale, dt, g->d_step, 0, g->st);
+        else
+            launch_overlap<float>((const float *const *)fp, g->nx, g->ny, g->d_jobs, g->njobs, g->job_cells,
+                                  g->d_partials, scale, dt, g->d_step, 0, g->st);
     }
     for (auto &b : g->binds) {
         TaperDev *td = nullptr;
@@ -936,6 +940,7 @@ bool enqueue_after_step(Grid *g, double dt)
         t.f = fp;
         t.nx = g->nx; t.ny = g->ny;
         t.jobs = g->d_jobs; t.njobs = g->njobs;
+        t.cells = g->job_cells;
         t.partials = g->d_partials;
         t.scale = scale; t.dt = dt;
         t.step = g->d_step;
@@ -964,9 +969,12 @@ bool rebuild_jobs(Grid *g)
         j.acc = mn.d_acc;
         j.omega = mn.d_omega;
         j.nfreq = mn.nfreq;
+        j.win = mode_window(g->nx, g->ny, j.cx, j.cy, j.mi, j.mj, j.ratio);
         jobs.push_back(j);
     }
     g->njobs = (int)jobs.size();
+    g->job_cells = 0;
+    for (auto &j : jobs) g->job_cells = std::max(g->job_cells, (long long)j.win.wni * j.win.wnj);
     if (g->njobs)
         CK(cudaMemcpyAsync(g->d_jobs, jobs.data(), jobs.size() * sizeof(OverlapJob), cudaMemcpyHostToDevice, g->st));
     g->version++;
@@ -1138,11 +1146,20 @@ static bool run_steps_in(Grid *g, double dt, int nsteps)
             note_launch((int)g->graph_nodes[0]);
         }
     } else if (full > 0) {
-        // two graphs alternate: while one runs, the host reads the other's
-        // event times, so the device never waits for the host
+        // One replay in g->ktime runs a timed graph, the others the plain one
+        // (the event records of a timed graph stand between the step's
+        // kernels, which then cannot overlap their launches).  Two timed
+        // graphs alternate: while one runs, the host reads the other's event
+        // times, so the device never waits for the host.
         if (!capture_graph(g, 1, dt) || !capture_graph(g, 2, dt)) return false;
-        for (int r = 0; r < full; r++) {
-            int set = r & 1;
+        if (g->ktime > 1 && !capture_graph(g, 0, dt)) return false;
+        for (int r = 0; r < full; r++, g->kreplay++) {
+            if (g->kreplay % g->ktime != 0) {
+                CK(cudaGraphLaunch(g->graph[0], g->st));
+                note_launch((int)g->graph_nodes[0]);
+                continue;
+            }
+            const int set = (int)((g->kreplay / g->ktime) & 1);
             if (!drain_kernel_timing(g, set)) return false;
             CK(cudaGraphLaunch(g->graph[1 + set], g->st));
             note_launch((int)g->graph_nodes[1 + set]);

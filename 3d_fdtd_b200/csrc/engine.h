@@ -134,6 +134,7 @@ struct Grid {
     long long host_steps = 0;
     OverlapJob *d_jobs = nullptr;       // monitors
     int jobs_cap = 0, njobs = 0;
+    long long job_cells = 0;        // largest overlap window of the jobs
     OverlapJob *d_job1 = nullptr;       // single compat overlap
     double2 *d_partials = nullptr;
     double2 *d_inst = nullptr;
@@ -169,8 +170,10 @@ struct Grid {
     long long graph_nodes[3] = {};      // kernel launches per replay
     uint64_t version = 1;               // bumped on any configuration change
 
-    // kernel timing: an event pair around the Yee update of every captured step
-    bool ktime = false;
+    // kernel timing: an event pair around the Yee update of every captured
+    // step of one graph replay in `ktime` (0: off)
+    int ktime = 0;
+    long long kreplay = 0;              // graph replays since timing was set
     cudaEvent_t kev[2][64] = {};        // per timed graph, 2 per step
     bool kpending[2] = {false, false};
     cudaEvent_t *cap_ev = nullptr;      // events of the graph being captured

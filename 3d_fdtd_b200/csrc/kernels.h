@@ -1,6 +1,8 @@
 // kernels.h -- host-side launchers of the device kernels (internal header).
 #pragma once
 
+#include <cmath>
+
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -11,6 +13,46 @@ namespace fdtd {
 // host-side count of kernel launches issued by this library (engine.cu)
 void note_launch(int n = 1);
 long long launch_count();
+
+// Cells [wi, wi + wni) x [wj, wj + wnj) of an nx x ny plane outside which no
+// cell maps to a sample of an mi x mj mode centred on (cx, cy) with ratio
+// r = grid disc / mode disc: along x the sample index (int)((i - cx) r) + mi/2
+// lies in [0, mi) only when -(mi/2) - 1 < (i - cx) r < mi - mi/2 (truncation
+// toward zero), and likewise along y.  The window keeps two cells of margin
+// beyond those bounds, so it is a superset under any rounding of the product;
+// the kernels still test every cell, so the window only removes work.
+struct ModeWindow {
+    int wi, wj, wni, wnj;
+};
+
+inline void mode_window_axis(int n, int c, int m, double r, int &lo, int &cnt)
+{
+    if (!(r > 0) || !std::isfinite(r)) {   // no usable bound: the whole axis
+        lo = 0;
+        cnt = n;
+        return;
+    }
+    double a = c + std::floor((double)(-(m / 2) - 1) / r) - 1;
+    double b = c + std::ceil((double)(m - m / 2) / r) + 1;
+    if (a < 0) a = 0;
+    if (b > n - 1) b = n - 1;
+    if (b < a) {
+        lo = 0;
+        cnt = 0;
+        return;
+    }
+    lo = (int)a;
+    cnt = (int)(b - a) + 1;
+}
+
+inline ModeWindow mode_window(int nx, int ny, int cx, int cy, int mi, int mj, double r)
+{
+    ModeWindow w{};
+    mode_window_axis(nx, cx, mi, r, w.wi, w.wni);
+    mode_window_axis(ny, cy, mj, r, w.wj, w.wnj);
+    if (w.wni == 0 || w.wnj == 0) w.wni = w.wnj = 0;
+    return w;
+}
 
 // one overlap reduction: plane cz of the grid against a device mode
 struct OverlapJob {
@@ -23,6 +65,7 @@ struct OverlapJob {
     double2 *acc;           // per-frequency (sum, compensation) pairs (or null)
     const double *omega;    // n_freq angular frequencies
     int nfreq;
+    ModeWindow win;         // mode_window of (cx, cy, mi, mj, ratio)
 };
 
 // plane source written from a complex mode (timefield3d_mode_source and
@@ -37,6 +80,7 @@ struct SourceJob {
     const double *sched;
     int nsched;
     int reverse, adjoint;
+    ModeWindow win;             // set by launch_mode_source_job / the tail launcher
 };
 
 // one launch at the end of a run step: overlap monitors of the step, the
@@ -46,6 +90,7 @@ struct TailArgs {
     int nx, ny;
     const OverlapJob *jobs;
     int njobs, nparts;
+    long long cells;            // largest overlap window of the jobs (cells)
     double2 *partials;
     double scale, dt;
     long long *step;
@@ -147,10 +192,12 @@ void launch_mode_source_job(const SourceJob &sj, double amplitude, double cph, d
 template <typename T>
 void launch_step_tail(TailArgs a, cudaStream_t st);
 void launch_set_value(float *p, long long idx, float v, cudaStream_t st);
-int overlap_parts(int nx, int ny);
+int overlap_parts(long long cells);
+// cells: the largest overlap window (win.wni * win.wnj) of the jobs
 template <typename T>
-void launch_overlap(const T *const *f_dev, int nx, int ny, const OverlapJob *jobs_dev, int njobs, double2 *partials,
-                    double scale, double dt, const long long *step, int step_offset, cudaStream_t st);
+void launch_overlap(const T *const *f_dev, int nx, int ny, const OverlapJob *jobs_dev, int njobs, long long cells,
+                    double2 *partials, double scale, double dt, const long long *step, int step_offset,
+                    cudaStream_t st);
 template <typename T>
 void launch_dft(const T *const *f_dev, int nx, int ny, int nz, int slice, int k_lo, int k_hi, double tr, double ti,
                 double2 *acc, cudaStream_t st);

@@ -452,12 +452,14 @@ __global__ void __launch_bounds__(kBlock4, W == 4 ? (SLABS ? 2 : 4) : 3) k_flat4
 template <bool E_FIELD, bool LOSSY>
 __global__ void __launch_bounds__(kBlock4, E_FIELD ? 3 : 4) k_flat4_merged(FlatArgs a, Plan4 p)
 {
-    // Programmatic dependent launch: every E block lets the H launch start
-    // scheduling (its blocks then fill SMs freed by the E tail); the H blocks
-    // wait here until the E grid has completed and its stores are visible.
-    // Both are no-ops in a launch without the attribute.
-    if (E_FIELD) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    else asm volatile("griddepcontrol.wait;" ::: "memory");
+    // Programmatic dependent launch: every block first waits until the
+    // preceding grid of the stream (the previous step's tail or H update, or
+    // the E update for H) has completed and its stores are visible, then lets
+    // the next launch start scheduling, so its blocks fill SMs freed by this
+    // grid's last wave and wait there in turn.  Both are no-ops in a launch
+    // without the attribute.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     int b = E_FIELD ? (int)blockIdx.x : (int)(gridDim.x - 1 - blockIdx.x);
     const int nzs = (p.L - 1) * p.nbz, nmb = p.nmid * p.nbm;
     int plane, lb;
@@ -594,7 +596,8 @@ void launch_flat4_step(const FlatArgs &a, cudaStream_t st, cudaStream_t side, cu
     const long long blocks = 2LL * (L - 1) * p.nbz + (long long)nmid * p.nbm;
     const bool lossy = a.ca[0] != nullptr;
     note_launch(2);
-    // H launch with a programmatic dependency on the E launch (see k_flat4_merged)
+    // both launches carry a programmatic dependency on the kernel before them
+    // (see k_flat4_merged)
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)blocks);
     cfg.blockDim = dim3(kBlock4);
@@ -605,10 +608,10 @@ void launch_flat4_step(const FlatArgs &a, cudaStream_t st, cudaStream_t side, cu
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     if (lossy) {
-        k_flat4_merged<true, true><<<(unsigned)blocks, kBlock4, 0, st>>>(a, p);
+        cudaLaunchKernelEx(&cfg, k_flat4_merged<true, true>, a, p);
         cudaLaunchKernelEx(&cfg, k_flat4_merged<false, true>, a, p);
     } else {
-        k_flat4_merged<true, false><<<(unsigned)blocks, kBlock4, 0, st>>>(a, p);
+        cudaLaunchKernelEx(&cfg, k_flat4_merged<true, false>, a, p);
         cudaLaunchKernelEx(&cfg, k_flat4_merged<false, false>, a, p);
     }
     (void)side; (void)fork; (void)join;

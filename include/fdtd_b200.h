@@ -396,9 +396,11 @@ int fdtd_wait_selftest(double limit_seconds, double *elapsed_seconds);
 void *timefield3d_get_stream(timefield3d psi);
 /* upload psi.ep/mu/sig now (otherwise done on the next device use after a change) */
 int timefield3d_upload_materials(timefield3d psi);
-/* Kernel timing: while on, every captured step of timefield3d_run records a CUDA
- * event pair around its Yee update (E and H kernels, boundary included); read
- * returns the summed milliseconds and the number of timed steps, then resets. */
+/* Kernel timing: while on (on = k > 0), every captured step of one graph
+ * replay of timefield3d_run in k records a CUDA event pair around its Yee
+ * update (E and H kernels, boundary included); the other replays run without
+ * events.  on = 0 turns it off; negative is an argument error.  Read returns
+ * the summed milliseconds and the number of timed steps, then resets. */
 int timefield3d_set_kernel_timing(timefield3d psi, int on);
 int timefield3d_read_kernel_timing(timefield3d psi, double *total_ms, long long *count);
 

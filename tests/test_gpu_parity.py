@@ -282,26 +282,28 @@ def test_wg_adjoint_gradient_golden(fd, orc, gpu):
 
 
 def test_kernel_timing_run_equals_untimed(fd, gpu):
-    """Timed graphs (event pairs around each Yee update) compute the same fields."""
+    """Timed graphs (event pairs around each Yee update), on every replay or on
+    one replay in 3, compute the same fields as the untimed run."""
     outs = []
-    for timed in (False, True):
+    # 100 steps = 3 graph replays of 32 steps + 4 single steps
+    for period, timed_steps in ((0, 0), (1, 96), (3, 32)):
         grid = fd.Grid(24, 20, 28, 0.02, fd.F32)
         lossy_problem(fd.lib, grid.t)
         fd.call("timefield3d_set_cpml", grid.t, 4, 3, -1.0, 1.0, 0.0)
         fd.call("timefield3d_set_source_value", grid.t, 10, 9, 14, 2, 1.0)
-        fd.call("timefield3d_set_kernel_timing", grid.t, int(timed))
+        fd.call("timefield3d_set_kernel_timing", grid.t, period)
         l0 = fd.lib.fdtd_launch_count()
         fd.call("timefield3d_run", grid.t, DT_FACTOR * 0.02, 100)
         ms, cnt = C.c_double(), C.c_longlong()
         fd.call("timefield3d_read_kernel_timing", grid.t, C.byref(ms), C.byref(cnt))
         launches = fd.lib.fdtd_launch_count() - l0
         assert launches >= 100 * 2
-        if timed:
-            assert cnt.value == 96 and ms.value > 0
-        else:
-            assert cnt.value == 0
+        assert cnt.value == timed_steps
+        assert (ms.value > 0) == (timed_steps > 0)
         outs.append(grid.fields())
-    assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+    assert fd.lib.timefield3d_set_kernel_timing(grid.t, -1) == fd.FDTD_ERR_ARG
+    fd.lib.fdtd_clear_error()
 
 
 def test_run_graph_equals_stepwise(fd, gpu):

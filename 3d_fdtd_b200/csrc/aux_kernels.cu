@@ -4,68 +4,9 @@
 // All of it touches one z-plane (or a list of edge cells) per step, so it is
 // a small fraction of a step's HBM traffic; what matters is that it stays on
 // the device (no per-step host round trip) and that the reductions are FP64.
-#include "common.cuh"
-#include "kernels.h"
+#include "plane_ops.cuh"
 
 namespace fdtd {
-
-// ---------------------------------------------------------------------------
-// Mode plane source, timefield3d_mode_source (timefield3d.c:2977-3026):
-//   src[m<3]  = A ep_m (Re cos(phase) + Im sin(phase))
-//   src[m>=3] = -M_sign A mu_m (Re cos(phase) + Im sin(phase)),  M_sign = 2 reverse - 1
-// from the mode sample at ((int)((i-cx) r) + mi/2, (int)((j-cy) r) + mj/2),
-// r = disc / mode.disc; cells whose sample falls outside the mode keep their
-// value.  Adjoint variant, timefield3d_mode_source_adjoint
-// (timefield3d.c:3028-3068): J = (Hy_m, -Hx_m, 0), M = (-M_sign Ey_m, M_sign Ex_m, 0).
-// cos/sin of the phase are computed on the host with the C library, like the
-// reference, and passed in; sched != null selects per-step values indexed by
-// the device step counter.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void schedule_values(const SourceJob &sj, long long n, double &A, double &c, double &s)
-{
-    if (n < 0 || n >= sj.nsched) {
-        A = 0.0; c = 0.0; s = 0.0;   // outside the schedule: zero source
-    } else {
-        A = sj.sched[3 * n]; c = sj.sched[3 * n + 1]; s = sj.sched[3 * n + 2];
-    }
-}
-
-// window cells u = first, first + stride, ... of the source plane
-__device__ __forceinline__ void mode_source_cells(const SourceJob &sj, long long first, long long stride, double A,
-                                                  double c, double s)
-{
-    const int nx = sj.nx;
-    const long long nxy = (long long)nx * sj.ny;
-    const int M_sign = -1 + 2 * sj.reverse;
-    float *plane = sj.plane;
-    const long long cells = (long long)sj.win.wni * sj.win.wnj;
-    for (long long u = first; u < cells; u += stride) {
-        const int i = sj.win.wi + (int)(u % sj.win.wni), j = sj.win.wj + (int)(u / sj.win.wni);
-        const long long t = i + (long long)nx * j;
-        double xd = dmul((double)(i - sj.cx), sj.ratio);
-        double yd = dmul((double)(j - sj.cy), sj.ratio);
-        int mx = (int)xd + sj.mi / 2, my = (int)yd + sj.mj / 2;
-        if (mx < 0 || mx >= sj.mi || my < 0 || my >= sj.mj) continue;
-        const double2 *e = sj.mode + 6LL * (mx + (long long)sj.mi * my);
-        if (!sj.adjoint) {
-#pragma unroll
-            for (int m = 0; m < 6; m++) {
-                double proj = dadd(dmul(e[m].x, c), dmul(e[m].y, s));
-                double v;
-                if (m < 3) v = dmul(dmul(A, (double)sj.ep[m][t]), proj);
-                else v = dmul(dmul(dmul((double)(-M_sign), A), (double)sj.mu[m - 3][t]), proj);
-                plane[m * nxy + t] = __double2float_rn(v);
-            }
-        } else {
-            plane[0 * nxy + t] = __double2float_rn(dmul(1.0, dadd(dmul(e[4].x, c), dmul(e[4].y, s))));
-            plane[1 * nxy + t] = __double2float_rn(dmul(-1.0, dadd(dmul(e[3].x, c), dmul(e[3].y, s))));
-            plane[2 * nxy + t] = 0.0f;
-            plane[3 * nxy + t] = __double2float_rn(dmul((double)(-1 * M_sign), dadd(dmul(e[1].x, c), dmul(e[1].y, s))));
-            plane[4 * nxy + t] = __double2float_rn(dmul((double)(1 * M_sign), dadd(dmul(e[0].x, c), dmul(e[0].y, s))));
-            plane[5 * nxy + t] = 0.0f;
-        }
-    }
-}
 
 // fixed amplitude and phase, or (sched != null) the schedule entry of step *step + offset
 __global__ void k_mode_source(SourceJob sj, double amplitude, double cph, double sph, const long long *step,
@@ -78,98 +19,12 @@ __global__ void k_mode_source(SourceJob sj, double amplitude, double cph, double
 
 __global__ void k_set_value(float *p, long long idx, float v) { p[idx] = v; }
 
-// ---------------------------------------------------------------------------
-// Mode overlap (timefield3d.c:3176-3233): per cell with a mode sample,
-//   Hx mEy - Hy mEx + Ey mHx - Ex mHy   (mode H -> -conj(H) when reverse)
-// summed over the plane in FP64.  One grid covers several monitors
-// (blockIdx.y); each block writes one partial; the finalize kernel adds the
-// partials in a fixed order (deterministic), scales by -dx^2/2 and, for
-// monitors, accumulates e^{i omega n dt} o(n) per frequency with Kahan
-// compensation.
-// ---------------------------------------------------------------------------
-// partial `part` of `nparts` of one job's plane sum, written to *out (all
-// threads of the block call it)
-template <typename T>
-__device__ __forceinline__ void overlap_block(const T *const *Ex_, int nx, int ny, const OverlapJob &jb, int part,
-                                              int nparts, double2 *out)
-{
-    const long long nxy = (long long)nx * ny;
-    const T *Ex = Ex_[0], *Ey = Ex_[1], *Hx = Ex_[3], *Hy = Ex_[4];
-    const long long base = nxy * jb.cz;
-    const long long cells = (long long)jb.win.wni * jb.win.wnj;
-    double sre = 0.0, sim = 0.0;
-    for (long long u = part * (long long)blockDim.x + threadIdx.x; u < cells; u += (long long)nparts * blockDim.x) {
-        const int i = jb.win.wi + (int)(u % jb.win.wni), j = jb.win.wj + (int)(u / jb.win.wni);
-        const long long t = i + (long long)nx * j;
-        double xd = dmul((double)(i - jb.cx), jb.ratio);
-        double yd = dmul((double)(j - jb.cy), jb.ratio);
-        int mx = (int)xd + jb.mi / 2, my = (int)yd + jb.mj / 2;
-        if (mx < 0 || mx >= jb.mi || my < 0 || my >= jb.mj) continue;
-        const double2 *e = jb.mode + 6LL * (mx + (long long)jb.mi * my);
-        double2 mEx = e[0], mEy = e[1], mHx = e[3], mHy = e[4];
-        if (jb.reverse) {
-            mHx.x = -mHx.x;
-            mHy.x = -mHy.x;
-        }
-        double ex = (double)Ex[base + t], ey = (double)Ey[base + t];
-        double hx = (double)Hx[base + t], hy = (double)Hy[base + t];
-        double re = dadd(dsub(dmul(hx, mEy.x), dmul(hy, mEx.x)), dsub(dmul(ey, mHx.x), dmul(ex, mHy.x)));
-        double im = dadd(dsub(dmul(hx, mEy.y), dmul(hy, mEx.y)), dsub(dmul(ey, mHx.y), dmul(ex, mHy.y)));
-        sre = dadd(sre, re);
-        sim = dadd(sim, im);
-    }
-    // warp then block reduction, fixed shape
-    for (int o = 16; o > 0; o >>= 1) {
-        sre = dadd(sre, __shfl_down_sync(0xffffffffu, sre, o));
-        sim = dadd(sim, __shfl_down_sync(0xffffffffu, sim, o));
-    }
-    __shared__ double2 ws[32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) ws[warp] = make_double2(sre, sim);
-    __syncthreads();
-    if (warp == 0) {
-        int nw = blockDim.x >> 5;
-        double2 v = lane < nw ? ws[lane] : make_double2(0.0, 0.0);
-        for (int o = 16; o > 0; o >>= 1) {
-            v.x = dadd(v.x, __shfl_down_sync(0xffffffffu, v.x, o));
-            v.y = dadd(v.y, __shfl_down_sync(0xffffffffu, v.y, o));
-        }
-        if (lane == 0) *out = v;
-    }
-}
-
 template <typename T>
 __global__ void k_overlap_partial(const T *const *Ex_, int nx, int ny, const OverlapJob *jobs, double2 *partials,
                                   int nparts)
 {
     const OverlapJob jb = jobs[blockIdx.y];
     overlap_block<T>(Ex_, nx, ny, jb, blockIdx.x, nparts, partials + (long long)blockIdx.y * nparts + blockIdx.x);
-}
-
-// reduce_phase: phase - (int)(phase/(2 pi)) 2 pi with the reference's 9-digit pi
-// (timefield3d.c:3,3235)
-__device__ __forceinline__ double reduce_phase(double ph)
-{
-    const double two_pi = dmul(2.0, 3.141592652);
-    double q = (double)(int)__ddiv_rn(ph, two_pi);
-    return dsub(ph, dmul(q, two_pi));
-}
-
-// acc[2f] += e^{i omega_f n dt} o with Kahan compensation in acc[2f+1]
-__device__ __forceinline__ void accumulate_frequency(const OverlapJob &jb, int f, double2 o, double dt, long long n)
-{
-    double ph = reduce_phase(dmul(dmul((double)n, dt), jb.omega[f]));
-    double s, c;
-    sincos(ph, &s, &c);
-    double add_re = dsub(dmul(c, o.x), dmul(s, o.y));
-    double add_im = dadd(dmul(c, o.y), dmul(s, o.x));
-    double2 sum = jb.acc[2 * f], comp = jb.acc[2 * f + 1];
-    double yr = dsub(add_re, comp.x), yi = dsub(add_im, comp.y);
-    double tr = dadd(sum.x, yr), ti = dadd(sum.y, yi);
-    comp.x = dsub(dsub(tr, sum.x), yr);
-    comp.y = dsub(dsub(ti, sum.y), yi);
-    jb.acc[2 * f] = make_double2(tr, ti);
-    jb.acc[2 * f + 1] = comp;
 }
 
 // sum one job's partials in order, scale, store the instantaneous value and

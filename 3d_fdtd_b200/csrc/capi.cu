@@ -797,12 +797,29 @@ int timefield3d_set_yee_variant(timefield3d psi, int variant)
     LOCK;
     Grid *g = grid_lookup(psi);
     if (!g) return FDTD_ERR_ARG;
-    if (variant < FDTD_YEE_AUTO || variant > FDTD_YEE_FLAT4) {
+    if (variant < FDTD_YEE_AUTO || variant > FDTD_YEE_WAVE) {
         set_error(FDTD_ERR_ARG, "yee variant %d", variant);
         return FDTD_ERR_ARG;
     }
     g->yee_variant = variant;
     g->version++;
+    return FDTD_OK;
+}
+
+int timefield3d_set_wave_steps(timefield3d psi, int steps_per_launch, int steps_per_sweep, int blocks_per_ticket)
+{
+    LOCK;
+    Grid *g = grid_lookup(psi);
+    if (!g) return FDTD_ERR_ARG;
+    if (steps_per_launch < 1 || steps_per_launch > 4096 || steps_per_sweep < 1 ||
+        steps_per_sweep > steps_per_launch || blocks_per_ticket < 1 || blocks_per_ticket > 64) {
+        set_error(FDTD_ERR_ARG, "wave steps %d per launch, %d per sweep, %d blocks per ticket", steps_per_launch,
+                  steps_per_sweep, blocks_per_ticket);
+        return FDTD_ERR_ARG;
+    }
+    g->wave.steps = steps_per_launch;
+    g->wave.sweep = steps_per_sweep;
+    g->wave.group = blocks_per_ticket;
     return FDTD_OK;
 }
 

@@ -356,6 +356,10 @@ Grid::~Grid()
         for (auto &p : planes) dfree(p.p);
         for (auto p : plane_pool) dfree(p);
         dfree(d_step); dfree(d_done); dfree(d_jobs); dfree(d_job1); dfree(d_partials); dfree(d_inst);
+        dfree(wave.d_items); dfree(wave.d_cnt); dfree(wave.d_part); dfree(wave.d_ring);
+        for (int s = 0; s < 2; s++)
+            for (int e = 0; e < 2; e++)
+                if (wave.ev[s][e]) cudaEventDestroy(wave.ev[s][e]);
         if (h_inst) cudaFreeHost(h_inst);
         if (h_flag) cudaFreeHost(h_flag);
         if (h_err) cudaFreeHost(h_err);
@@ -859,7 +863,7 @@ template <typename T> static bool step_split(Grid *g, double dt)
     return true;
 }
 
-static bool step_flat(Grid *g, double dt)
+static FlatArgs flat_args(Grid *g, double dt)
 {
     FlatArgs a{};
     a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
@@ -873,6 +877,14 @@ static bool step_flat(Grid *g, double dt)
         for (int w = 0; w < 6; w++) a.prof[w][ax] = (const float *)g->prof[w][ax];
     }
     a.src = source_table(g);
+    a.ring = nullptr;
+    a.ring_k = -1;
+    return a;
+}
+
+static bool step_flat(Grid *g, double dt)
+{
+    const FlatArgs a = flat_args(g, dt);
     const bool four = g->yee_variant != FDTD_YEE_FLAT && flat4_supported(g->nx, g->nz);
     if (four) launch_flat4_step(a, g->st, g->side, g->ev_fork, g->ev_join);
     else launch_flat_step(a, g->st, nullptr);
@@ -973,6 +985,8 @@ bool rebuild_jobs(Grid *g)
         jobs.push_back(j);
     }
     g->njobs = (int)jobs.size();
+    g->job_z.clear();
+    for (auto &j : jobs) g->job_z.push_back(j.cz);
     g->job_cells = 0;
     for (auto &j : jobs) g->job_cells = std::max(g->job_cells, (long long)j.win.wni * j.win.wnj);
     if (g->njobs)
@@ -1026,6 +1040,114 @@ bool enqueue_step(Grid *g, double dt, bool with_extras)
     if (!ok) return false;
     if (g->cap_ev) CK(cudaEventRecordWithFlags(g->cap_ev[2 * g->cap_step + 1], g->st, cudaEventRecordExternal));
     return with_extras ? enqueue_after_step(g, dt) : true;
+}
+
+// ============================================================================
+// multi-step wavefront launches (FDTD_YEE_WAVE)
+// ============================================================================
+// A run's full chunks go through one wavefront launch per chunk when the grid
+// is on the FP32 flat4 path and the run carries nothing that needs per-step
+// kernels (probes, taper stores); monitors and the scheduled source are
+// handled inside (their planes must be updated planes, 1..nz-2).
+static bool wave_path(Grid *g, double dt)
+{
+    if (!fast32_path(g) || g->yee_variant != FDTD_YEE_WAVE) return false;
+    if (!flat4_supported(g->nx, g->nz) || !g->probes.empty() || !g->binds.empty()) return false;
+    const FlatArgs a = flat_args(g, dt);
+    if (a.L > 0 && !flat4_split_supported(a)) return false;
+    for (int z : g->job_z)
+        if (z < 1 || z > g->nz - 2) return false;
+    if (g->sched.active && (g->sched.cz < 1 || g->sched.cz > g->nz - 2)) return false;
+    return true;
+}
+
+// (re)build the wavefront tables for the grid's current configuration
+static bool wave_tables(Grid *g, const Plan4 &p)
+{
+    auto &w = g->wave;
+    const int sched_k = g->sched.active ? g->sched.cz : -1;
+    if (w.version == g->version && w.built_steps == w.steps && w.built_sweep == w.sweep && w.built_group == w.group &&
+        w.built_sched_k == sched_k && w.d_items)
+        return true;
+    CK(cudaStreamSynchronize(g->st));
+    dfree(w.d_items); dfree(w.d_cnt); dfree(w.d_part); dfree(w.d_ring);
+    w.nparts = g->njobs ? overlap_parts(g->job_cells) : 1;
+    if (wave_items(p, g->nz, w.steps, w.sweep, w.group, g->job_z.data(), g->njobs, w.nparts, w.items, w.tickets) !=
+        0) {
+        set_error(FDTD_ERR_ARG, "wavefront run: sizes out of range");
+        return false;
+    }
+    for (int l = 0; l < 2; l++) {
+        if (!w.grid[l]) w.grid[l] = wave_grid(l == 1);
+        if (w.grid[l] <= 0) {
+            set_error(FDTD_ERR_CUDA, "wavefront run: kernel cannot be resident on this device");
+            return false;
+        }
+    }
+    const long long nxy = (long long)g->nx * g->ny;
+    if (!dalloc(&w.d_items, w.items.size() * sizeof(WaveItem), g->st, false)) return false;
+    if (!dalloc(&w.d_cnt, ((size_t)wave_counters(g->nz, w.steps) + 1) * sizeof(unsigned), g->st)) return false;
+    if (!dalloc(&w.d_part, (size_t)w.steps * std::max(1, g->njobs) * w.nparts * sizeof(double2), g->st)) return false;
+    if (sched_k >= 0 && !dalloc(&w.d_ring, (size_t)w.steps * 6 * nxy * sizeof(float), g->st, false)) return false;
+    CK(cudaMemcpyAsync(w.d_items, w.items.data(), w.items.size() * sizeof(WaveItem), cudaMemcpyHostToDevice, g->st));
+    w.version = g->version;
+    w.built_steps = w.steps;
+    w.built_sweep = w.sweep;
+    w.built_group = w.group;
+    w.built_sched_k = sched_k;
+    return true;
+}
+
+// one wavefront launch of g->wave.steps steps; `timed`: event pair `set` around it
+static bool enqueue_wave(Grid *g, double dt, bool timed, int set)
+{
+    FlatArgs a = flat_args(g, dt);
+    const Plan4 p = flat4_plan(a);
+    if (!wave_tables(g, p)) return false;
+    auto &w = g->wave;
+    WaveArgs wa{};
+    wa.items = w.d_items;
+    wa.nitems = (int)w.items.size();
+    wa.tickets = w.tickets;
+    wa.cnt = w.d_cnt;
+    wa.next = w.d_cnt + wave_counters(g->nz, w.steps);
+    wa.nz = g->nz;
+    wa.steps = w.steps;
+    wa.jobs = g->d_jobs;
+    wa.njobs = g->njobs;
+    wa.nparts = w.nparts;
+    wa.partials = w.d_part;
+    wa.group = w.group;
+    wa.err = g->d_err;
+    wa.wait_ns = 1000000000ull;
+    WaveFinal fin{};
+    fin.jobs = g->d_jobs;
+    fin.njobs = g->njobs;
+    fin.nparts = w.nparts;
+    fin.steps = w.steps;
+    fin.partials = w.d_part;
+    fin.scale = (-0.5 * g->dx * g->dx);
+    fin.dt = dt;
+    fin.step = g->d_step;
+    fin.done = g->d_done;
+    SourceJob sj{};
+    if (g->sched.active) {
+        if (!schedule_job(g, &sj)) return false;
+        fin.src = sj;
+        a.ring_k = g->sched.cz;
+    }
+    if (timed) {
+        for (int e = 0; e < 2; e++)
+            if (!w.ev[set][e]) CK(cudaEventCreate(&w.ev[set][e]));
+        CK(cudaEventRecord(w.ev[set][0], g->st));
+    }
+    CK(launch_wave(a, p, wa, w.grid[a.ca[0] ? 1 : 0], g->sched.active ? &sj : nullptr, w.d_ring, fin, g->st));
+    if (timed) {
+        CK(cudaEventRecord(w.ev[set][1], g->st));
+        w.pending[set] = true;
+        w.timed_steps[set] = w.steps;
+    }
+    return true;
 }
 
 static bool prepare_run(Grid *g, double dt)
@@ -1103,9 +1225,19 @@ static bool capture_graph(Grid *g, int slot, double dt)
     return true;
 }
 
-// read the Yee-update times of timed graph `set` once it has completed
+// read the Yee-update times of timed graph (or wavefront launch) `set` once
+// it has completed
 bool drain_kernel_timing(Grid *g, int set)
 {
+    auto &w = g->wave;
+    if (w.pending[set]) {
+        CK(cudaEventSynchronize(w.ev[set][1]));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, w.ev[set][0], w.ev[set][1]));
+        g->ktime_ms += ms;
+        g->ktime_n += w.timed_steps[set];
+        w.pending[set] = false;
+    }
     if (!g->kpending[set]) return true;
     CK(cudaEventSynchronize(g->kev[set][2 * kGraphSteps - 1]));
     for (int s = 0; s < kGraphSteps; s++) {
@@ -1138,6 +1270,20 @@ bool run_steps(Grid *g, double dt, int nsteps)
 
 static bool run_steps_in(Grid *g, double dt, int nsteps)
 {
+    if (nsteps >= g->wave.steps && wave_path(g, dt)) {
+        // wavefront launches of wave.steps steps; one in g->ktime timed
+        const int full = nsteps / g->wave.steps, rest = nsteps % g->wave.steps;
+        for (int r = 0; r < full; r++, g->kreplay++) {
+            const bool timed = g->ktime > 0 && g->kreplay % g->ktime == 0;
+            const int set = g->ktime > 0 ? (int)((g->kreplay / g->ktime) & 1) : 0;
+            if (timed && !drain_kernel_timing(g, set)) return false;
+            if (!enqueue_wave(g, dt, timed, set)) return false;
+        }
+        for (int s = 0; s < rest; s++)
+            if (!enqueue_step(g, dt, true)) return false;
+        g->host_steps += nsteps;
+        return true;
+    }
     int full = nsteps / kGraphSteps, rest = nsteps % kGraphSteps;
     if (full > 0 && !g->ktime) {
         if (!capture_graph(g, 0, dt)) return false;

@@ -181,6 +181,25 @@ struct Grid {
     double ktime_ms = 0;
     long long ktime_n = 0;
 
+    // multi-step wavefront launches (FDTD_YEE_WAVE, yee_wave.cu)
+    struct Wave {
+        int steps = 64, sweep = 16, group = 2;  // steps per launch, steps per sweep, blocks per ticket
+        // configuration the device tables were built for
+        uint64_t version = 0;
+        int built_steps = 0, built_sweep = 0, built_group = 0, built_sched_k = -2;
+        std::vector<WaveItem> items;        // kept: the source of the asynchronous upload
+        WaveItem *d_items = nullptr;
+        int tickets = 0, nparts = 1;
+        unsigned *d_cnt = nullptr;
+        double2 *d_part = nullptr;
+        float *d_ring = nullptr;
+        int grid[2] = {0, 0};               // co-resident blocks: lossless, lossy
+        cudaEvent_t ev[2][2] = {};          // kernel timing: one pair per timed launch
+        bool pending[2] = {false, false};
+        int timed_steps[2] = {0, 0};
+    } wave;
+    std::vector<int> job_z;               // plane of each overlap job (d_jobs order)
+
     ~Grid();
 };
 

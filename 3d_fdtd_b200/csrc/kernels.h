@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cmath>
+#include <vector>
 
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -130,6 +131,11 @@ struct FusedArgs {
     float *psi_out[3][4];
     const float *prof[6][3];
     SourcePlanes src;
+    // multi-step launches: per-step copies of the scheduled source plane
+    // (plane ring_k), ring_stride floats apart; null otherwise
+    const float *ring;
+    int ring_k;
+    long long ring_stride;
 };
 int fused_supported(int nx, int ny, int nz);
 void launch_fused_step(const FusedArgs &a, cudaStream_t st);
@@ -145,6 +151,11 @@ struct FlatArgs {
     float *psi[3][4];
     const float *prof[6][3];
     SourcePlanes src;
+    // multi-step launches: per-step copies of the scheduled source plane
+    // (plane ring_k), ring_stride floats apart; null otherwise
+    const float *ring;
+    int ring_k;
+    long long ring_stride;
 };
 void launch_flat_step(const FlatArgs &a, cudaStream_t st, cudaEvent_t mid);
 int flat4_supported(int nx, int nz);
@@ -165,9 +176,57 @@ struct Plan4 {
     Region4 zs, box, yrows, xcols;
 };
 bool flat4_split_supported(const FlatArgs &a);
+// block plan of one field update: a CPML grid that splits (flat4_split_supported)
+// gets the regions above; a grid without CPML (L = 0) whole planes 1..nz-2 in zs
+// with W = 4, nbz blocks per plane
+Plan4 flat4_plan(const FlatArgs &a);
 // E then H update.  With a CPML and a side stream the interior box runs on `st`
 // and the shell on `side` (fork/join through the two events) for each field.
 void launch_flat4_step(const FlatArgs &a, cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join);
+
+// yee_wave.cu: S steps of the flat4 update in one persistent, cooperative
+// launch, wavefront-ordered in z (see the file's header)
+struct WaveItem {
+    int t0;          // first ticket
+    int desc;        // kind (0 E, 1 H, 2 overlaps) | plane << 2 | step << 17
+    int nblocks;     // blocks of work (a ticket takes up to `group` of them)
+    int pad;
+    int2 dep[3];     // {counter, finished tickets needed}; counter -1: none
+};
+struct WaveArgs {
+    const WaveItem *items;
+    int nitems, tickets;
+    unsigned *cnt;                // finished tickets per item, wave_counters(nz, steps)
+    unsigned *next;               // next ticket to hand out (cnt + wave_counters)
+    int nz, steps;
+    const OverlapJob *jobs;       // monitors (device)
+    int njobs, nparts;
+    double2 *partials;            // [step][job][part]
+    int group;                    // blocks of work per ticket
+    int *err;                     // set to 1 when a wait gives up
+    unsigned long long wait_ns;   // bound of one wait
+};
+struct WaveFinal {
+    const OverlapJob *jobs;
+    int njobs, nparts, steps;
+    const double2 *partials;
+    double scale, dt;
+    long long *step;
+    unsigned *done;               // completion count, 0 between launches
+    SourceJob src;                // scheduled source (plane null: none)
+};
+// item list in ticket order (a ticket: up to `group` blocks of work of one
+// item); job_z: plane of each monitor (all in 1..nz-2); returns 0, or -1 when
+// the sizes are out of range
+int wave_items(const Plan4 &p, int nz, int steps, int sweep, int group, const int *job_z, int njobs, int nparts,
+               std::vector<WaveItem> &out, int &tickets);
+int wave_counters(int nz, int steps);
+// co-resident blocks of the wavefront kernel on the current device (0: cannot run)
+int wave_grid(bool lossy);
+// counters reset, source ring (sched non-null; a.ring_k = its plane), the
+// wavefront launch, then the finalize kernel
+cudaError_t launch_wave(const FlatArgs &a, const Plan4 &p, const WaveArgs &w, int grid, const SourceJob *sched,
+                        float *ring, const WaveFinal &fin, cudaStream_t st);
 
 // yee_fused_tma.cu (the same step with TMA staging; needs nx % 4 == 0)
 struct FusedMaps {

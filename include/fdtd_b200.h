@@ -221,11 +221,18 @@ enum fdtd_status {
 };
 enum fdtd_precision { FDTD_F64 = 0, FDTD_F32 = 1 };
 /* FP32 grids with mu = 1, no magnetic loss and a CPML or PEC boundary run one of
- * three kernel designs: flat (one thread per cell, separate E and H launches),
+ * four kernel designs: flat (one thread per cell, separate E and H launches),
  * flat4 (separate E and H launches, four x cells per thread with 16-byte
- * accesses; nx % 4 == 0) or fused (one launch per step streaming z-planes through
- * shared memory).  AUTO picks flat4 where nx allows, else flat. */
-enum fdtd_yee_variant { FDTD_YEE_AUTO = 0, FDTD_YEE_FLAT = 1, FDTD_YEE_FUSED = 2, FDTD_YEE_FLAT4 = 3 };
+ * accesses; nx % 4 == 0), fused (one launch per step streaming z-planes through
+ * shared memory) or wave (flat4's cell updates, but timefield3d_run executes
+ * whole chunks of steps -- monitors and scheduled source included -- in one
+ * persistent launch ordered as a wavefront in z, so a sweep's planes stay in
+ * L2; runs with probes or bound taper stores, and single steps, use flat4).
+ * AUTO picks flat4 where nx allows, else flat.  wave's fields are
+ * bit-identical to flat4's. */
+enum fdtd_yee_variant {
+    FDTD_YEE_AUTO = 0, FDTD_YEE_FLAT = 1, FDTD_YEE_FUSED = 2, FDTD_YEE_FLAT4 = 3, FDTD_YEE_WAVE = 4
+};
 enum fdtd_boundary { FDTD_BOUNDARY_MUR = 0, FDTD_BOUNDARY_CPML = 1, FDTD_BOUNDARY_PEC = 2 };
 
 /* status of the last failing call on this thread (sticky until cleared) */
@@ -243,6 +250,23 @@ int timefield3d_set_precision(timefield3d psi, int precision);
 int timefield3d_set_boundary(timefield3d psi, int boundary);
 /* kernel design of the FP32 fast path (enum fdtd_yee_variant); results agree to FP32 rounding */
 int timefield3d_set_yee_variant(timefield3d psi, int variant);
+/* FDTD_YEE_WAVE: steps per persistent launch (default 64), steps per sweep
+ * (default 16; a sweep keeps about 4 x steps_per_sweep planes live) and blocks
+ * of work per ticket (default 2; a ticket's synchronisation is paid once per
+ * group).  No reference counterpart.  steps_per_launch in [1, 4096],
+ * steps_per_sweep in [1, steps_per_launch], blocks_per_ticket in [1, 64];
+ * anything else is FDTD_ERR_ARG. */
+int timefield3d_set_wave_steps(timefield3d psi, int steps_per_launch, int steps_per_sweep, int blocks_per_ticket);
+/* The work-item table of one FDTD_YEE_WAVE launch (host computation, no device
+ * work), for inspection and tests.  No reference counterpart.  Grid nx x ny x nz
+ * (nx % 4 == 0), CPML thickness (0: none), monitors on planes job_z[0..njobs),
+ * nparts overlap partials per monitor.  Writes 9 ints per item into out
+ * (capacity cap items; out may be null to count): first ticket, descriptor
+ * (kind 0 E / 1 H / 2 overlaps | plane << 2 | step << 17), blocks of work,
+ * then three (counter, required count) pairs, counter -1 for none.  Returns the item count
+ * and the ticket total, or -1 on invalid input. */
+int fdtd_wave_schedule(int nx, int ny, int nz, int cpml_cells, int steps, int sweep, int blocks_per_ticket,
+                       const int *job_z, int njobs, int nparts, int *out, int cap, int *tickets);
 /* CPML of `thickness` cells on every face, polynomial grading `order`;
  * sigma_max <= 0 selects 0.8 (order+1)/disc; kappa_max >= 1; alpha_max >= 0.
  * Profiles depend on delta_t and are rebuilt when the step size changes.

@@ -185,19 +185,31 @@ __device__ __forceinline__ double reduce_phase(double ph)
 }
 
 // acc[2f] += e^{i omega_f n dt} o with Kahan compensation in acc[2f+1]
-__device__ __forceinline__ void accumulate_frequency(const OverlapJob &jb, int f, double2 o, double dt, long long n)
+// e^{i omega_f n dt} o
+__device__ __forceinline__ double2 frequency_term(const OverlapJob &jb, int f, double2 o, double dt, long long n)
 {
     double ph = reduce_phase(dmul(dmul((double)n, dt), jb.omega[f]));
     double s, c;
     sincos(ph, &s, &c);
-    double add_re = dsub(dmul(c, o.x), dmul(s, o.y));
-    double add_im = dadd(dmul(c, o.y), dmul(s, o.x));
-    double2 sum = jb.acc[2 * f], comp = jb.acc[2 * f + 1];
-    double yr = dsub(add_re, comp.x), yi = dsub(add_im, comp.y);
+    return make_double2(dsub(dmul(c, o.x), dmul(s, o.y)), dadd(dmul(c, o.y), dmul(s, o.x)));
+}
+
+// sum += add with Kahan compensation comp
+__device__ __forceinline__ void kahan_add(double2 &sum, double2 &comp, double2 add)
+{
+    double yr = dsub(add.x, comp.x), yi = dsub(add.y, comp.y);
     double tr = dadd(sum.x, yr), ti = dadd(sum.y, yi);
     comp.x = dsub(dsub(tr, sum.x), yr);
     comp.y = dsub(dsub(ti, sum.y), yi);
-    jb.acc[2 * f] = make_double2(tr, ti);
+    sum = make_double2(tr, ti);
+}
+
+__device__ __forceinline__ void accumulate_frequency(const OverlapJob &jb, int f, double2 o, double dt, long long n)
+{
+    const double2 add = frequency_term(jb, f, o, dt, n);
+    double2 sum = jb.acc[2 * f], comp = jb.acc[2 * f + 1];
+    kahan_add(sum, comp, add);
+    jb.acc[2 * f] = sum;
     jb.acc[2 * f + 1] = comp;
 }
 

@@ -251,43 +251,73 @@ __global__ void k_wave_ring(SourceJob sj, float *ring, long long stride, const l
     }
 }
 
-// block 0: per monitor (one warp each) and step, the partials added in order,
-// scaled, and accumulated per frequency (the per-step tail's arithmetic and
-// order); blocks 1..: the scheduled source of step n0 + S into the plane
-// buffer; the last block to finish advances the step counter
+// blocks 0..njobs-1: one monitor each.  Per chunk of 32 steps, the step
+// totals (partials added in order, scaled) in parallel, then the terms
+// e^{i omega_f n dt} o(n) of every (step, frequency) in parallel, then per
+// frequency the Kahan additions in step order, the sums kept in registers
+// (the per-step tail's arithmetic and order).  Blocks njobs..: the scheduled
+// source of step n0 + S into the plane buffer.  The last block to finish
+// advances the step counter.
 __global__ void __launch_bounds__(256) k_wave_finalize(WaveFinal f)
 {
+    constexpr int CH = 32;   // steps per chunk, frequencies per pass
     const long long n0 = *f.step;
-    if (blockIdx.x == 0) {
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        for (int jid = warp; jid < f.njobs; jid += blockDim.x >> 5) {
-            const OverlapJob jb = f.jobs[jid];
-            for (int ls = 0; ls < f.steps; ls++) {
-                const double2 *pp = f.partials + ((long long)ls * f.njobs + jid) * f.nparts;
-                double sre = 0.0, sim = 0.0;
-                for (int q = 0; q < f.nparts; q++) {
-                    const double2 v = pp[q];
-                    sre = dadd(sre, v.x);
-                    sim = dadd(sim, v.y);
+    const int tid = threadIdx.x;
+    if ((int)blockIdx.x < f.njobs) {
+        __shared__ double2 tot[CH];
+        __shared__ double2 term[CH][CH];
+        const OverlapJob jb = f.jobs[blockIdx.x];
+        const double2 *pj = f.partials + (long long)blockIdx.x * f.nparts;
+        const long long pstride = (long long)f.njobs * f.nparts;   // one step further
+        for (int fb = 0; fb == 0 || (jb.acc && fb < jb.nfreq); fb += CH) {
+            const int fq = fb + tid;
+            const bool mine = tid < CH && jb.acc && fq < jb.nfreq;
+            double2 sum = make_double2(0.0, 0.0), comp = sum;
+            if (mine) {
+                sum = jb.acc[2 * fq];
+                comp = jb.acc[2 * fq + 1];
+            }
+            for (int c0 = 0; c0 < f.steps; c0 += CH) {
+                const int nl = min(CH, f.steps - c0);
+                if (tid < nl) {
+                    const double2 *pp = pj + (long long)(c0 + tid) * pstride;
+                    double sre = 0.0, sim = 0.0;
+                    for (int q = 0; q < f.nparts; q++) {
+                        const double2 v = pp[q];
+                        sre = dadd(sre, v.x);
+                        sim = dadd(sim, v.y);
+                    }
+                    tot[tid] = make_double2(dmul(f.scale, sre), dmul(f.scale, sim));
                 }
-                const double2 tot = make_double2(dmul(f.scale, sre), dmul(f.scale, sim));
-                if (lane == 0 && jb.inst) *jb.inst = tot;
+                __syncthreads();
                 if (jb.acc)
-                    for (int q = lane; q < jb.nfreq; q += 32) accumulate_frequency(jb, q, tot, f.dt, n0 + ls);
+                    for (int q = tid; q < CH * CH; q += blockDim.x) {
+                        const int l = q / CH, fi = q % CH;
+                        if (l < nl && fb + fi < jb.nfreq) term[l][fi] = frequency_term(jb, fb + fi, tot[l], f.dt, n0 + c0 + l);
+                    }
+                __syncthreads();
+                if (mine)
+                    for (int l = 0; l < nl; l++) kahan_add(sum, comp, term[l][tid]);
+                if (tid == 0 && fb == 0 && jb.inst && c0 + nl == f.steps) *jb.inst = tot[nl - 1];
+                __syncthreads();
+            }
+            if (mine) {
+                jb.acc[2 * fq] = sum;
+                jb.acc[2 * fq + 1] = comp;
             }
         }
-    } else {
+    } else if (f.src.plane) {
         double A, c, s;
         schedule_values(f.src, n0 + f.steps, A, c, s);
-        mode_source_cells(f.src, (blockIdx.x - 1) * (long long)blockDim.x + threadIdx.x,
-                          (long long)(gridDim.x - 1) * blockDim.x, A, c, s);
+        mode_source_cells(f.src, (blockIdx.x - f.njobs) * (long long)blockDim.x + tid,
+                          (long long)(gridDim.x - f.njobs) * blockDim.x, A, c, s);
     }
     __shared__ bool last;
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(f.done, 1u) == gridDim.x - 1;
+    if (tid == 0) last = atomicAdd(f.done, 1u) == gridDim.x - 1;
     __syncthreads();
-    if (last && threadIdx.x == 0) {
+    if (last && tid == 0) {
         *f.step = n0 + f.steps;
         *f.done = 0u;
     }
@@ -412,12 +442,13 @@ cudaError_t launch_wave(const FlatArgs &a, const Plan4 &p, const WaveArgs &w, in
                 : cudaLaunchKernelExC(&cfg, (const void *)k_wave<false>, args);
     if (e != cudaSuccess) return e;
     WaveFinal ff = fin;
-    int fin_blocks = 1;
+    int fin_blocks = ff.njobs;
     if (ff.src.plane) {
         ff.src.win = mode_window(ff.src.nx, ff.src.ny, ff.src.cx, ff.src.cy, ff.src.mi, ff.src.mj, ff.src.ratio);
         const long long cells = (long long)ff.src.win.wni * ff.src.win.wnj;
         fin_blocks += (int)std::min<long long>(std::max<long long>(1, (cells + 255) / 256), 1184);
     }
+    fin_blocks = std::max(fin_blocks, 1);   // one block at least, to advance the counter
     note_launch();
     k_wave_finalize<<<fin_blocks, 256, 0, st>>>(ff);
     return cudaGetLastError();

@@ -294,7 +294,7 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
     ranks = importlib.import_module("3d_fdtd_b200.replicas").Ranks("nccl", timeout_s=120)
     barrier, max_over_ranks = ranks.barrier, ranks.max
 
-    sim = Taper(fd, args.time_steps, {"auto": 0, "flat": 1, "fused": 2, "flat4": 3}[args.yee_variant])
+    sim = Taper(fd, args.time_steps, {"auto": 0, "flat": 1, "fused": 2, "flat4": 3, "wave": 4}[args.yee_variant])
     stream = torch.cuda.ExternalStream(fd.lib.timefield3d_get_stream(sim.t))
     cells = W["nx"] * W["ny"] * W["nz"]
     # warm-up: full runs (graph capture, clocks)
@@ -334,7 +334,8 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
     bytes_step = algorithmic_bytes_per_step(W["nx"], W["ny"], W["nz"], W["cpml"])
     achieved = bytes_step / (kms / 1e3) / 1e9
     peak, peak_kind = peaks()
-    kernel_tag = "yee_step_si_taper_200x160x400_fp32"
+    wave = args.yee_variant == "wave"
+    kernel_tag = "yee_wave_si_taper_200x160x400_fp32" if wave else "yee_step_si_taper_200x160x400_fp32"
     traffic = read_traffic(kernel_tag)
     # end to end through the public API, host clock
     barrier()
@@ -362,10 +363,12 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
                 "config": config_block(args),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                             "kernel": "Yee step (E and H update kernels, CPML terms)",
+                             "kernel": ("wavefront launch (E, H, CPML, source, monitor partials), per step"
+                                        if wave else "Yee step (E and H update kernels, CPML terms)"),
                              "bytes_per_launch": bytes_step, "avg_launch_ms": kms,
                              "timed_launches": kcnt.value,
-                             "timed_sample": f"Yee E+H of every step of one 32-step graph replay in {KTIME_PERIOD}"},
+                             "timed_sample": (f"one wavefront launch in {KTIME_PERIOD}" if wave else
+                                              f"Yee E+H of every step of one 32-step graph replay in {KTIME_PERIOD}")},
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e, "unit": "Mcell-updates/s", "h2d_bytes_per_step": sim.h2d_bytes(),
                         "d2h_bytes_per_step": sim.d2h_bytes()},
@@ -385,7 +388,7 @@ def main():
     ap.add_argument("--time-steps", type=int, default=W["time_steps"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--yee-variant", choices=["auto", "flat", "flat4", "fused"], default="auto")
+    ap.add_argument("--yee-variant", choices=["auto", "flat", "flat4", "fused", "wave"], default="auto")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -1468,25 +1468,29 @@ bool grid_checkpoint_save(Grid *g, const char *path)
     int hdr[9] = {g->nx, g->ny, g->nz, g->prec, g->boundary, g->L, (int)g->monitors.size(), (int)g->planes.size(),
                   has_psi ? 1 : 0};
     long long dstep = 0;
-    CK(cudaMemcpy(&dstep, g->d_step, sizeof(long long), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(&dstep, g->d_step, sizeof(long long), cudaMemcpyDeviceToHost, g->st));
+    CK(cudaStreamSynchronize(g->st));
     long long steps[2] = {g->host_steps, dstep};
     bool ok = wr(fc.f, "FDTDCKP1", 8) && wr(fc.f, hdr, sizeof hdr) && wr(fc.f, steps, sizeof steps);
     std::vector<char> buf;
     for (auto &mn : g->monitors) {
         buf.resize(2 * (size_t)mn.nfreq * sizeof(double2));
-        CK(cudaMemcpy(buf.data(), mn.d_acc, buf.size(), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(buf.data(), mn.d_acc, buf.size(), cudaMemcpyDeviceToHost, g->st));
+        CK(cudaStreamSynchronize(g->st));
         ok = ok && wr(fc.f, &mn.nfreq, sizeof(int)) && wr(fc.f, buf.data(), buf.size());
     }
     const size_t pb = 6 * (size_t)g->nx * g->ny * sizeof(float);
     for (auto &pl : g->planes) {
         buf.resize(pb);
-        CK(cudaMemcpy(buf.data(), pl.p, pb, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(buf.data(), pl.p, pb, cudaMemcpyDeviceToHost, g->st));
+        CK(cudaStreamSynchronize(g->st));
         ok = ok && wr(fc.f, &pl.k, sizeof(int)) && wr(fc.f, buf.data(), pb);
     }
     const size_t fb = (size_t)g->n * esize(g);
     buf.resize(fb);
     for (int m = 0; m < 6 && ok; m++) {
-        CK(cudaMemcpy(buf.data(), g->f[g->cur][m], fb, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(buf.data(), g->f[g->cur][m], fb, cudaMemcpyDeviceToHost, g->st));
+        CK(cudaStreamSynchronize(g->st));
         ok = wr(fc.f, buf.data(), fb);
     }
     if (has_psi) {
@@ -1495,7 +1499,8 @@ bool grid_checkpoint_save(Grid *g, const char *path)
         for (int a = 0; a < 3; a++)
             for (int w = 0; w < 4 && ok; w++) {
                 buf.resize(sz[a]);
-                CK(cudaMemcpy(buf.data(), g->psi[g->cur][a][w], sz[a], cudaMemcpyDeviceToHost));
+                CK(cudaMemcpyAsync(buf.data(), g->psi[g->cur][a][w], sz[a], cudaMemcpyDeviceToHost, g->st));
+                CK(cudaStreamSynchronize(g->st));
                 ok = wr(fc.f, buf.data(), sz[a]);
             }
     }
@@ -1508,6 +1513,11 @@ bool grid_checkpoint_save(Grid *g, const char *path)
 
 bool grid_checkpoint_load(Grid *g, const char *path)
 {
+    // The whole file is read and checked into host memory first; device state
+    // is written only once every part is known to be present and to fit this
+    // grid, so a refused or truncated file leaves the grid as it was.  Every
+    // write then goes on the grid's stream (after the allocations' zero fills
+    // on that stream) and is waited for before returning.
     if (!grid_ensure_device(g)) return false;
     CK(cudaStreamSynchronize(g->st));
     FileCloser fc{fopen(path, "rb")};
@@ -1532,46 +1542,88 @@ bool grid_checkpoint_load(Grid *g, const char *path)
                   g->L, (int)g->monitors.size());
         return false;
     }
-    std::vector<char> buf;
-    for (auto &mn : g->monitors) {
+    if (hdr[7] < 0 || hdr[7] > kMaxSourcePlanes || (hdr[8] && g->boundary != FDTD_BOUNDARY_CPML)) {
+        set_error(FDTD_ERR_ARG, "checkpoint: %s has %d source planes / CPML flag %d, not valid for this grid", path,
+                  hdr[7], hdr[8]);
+        return false;
+    }
+    // ---- read everything
+    std::vector<std::vector<char>> acc(g->monitors.size());
+    for (size_t q = 0; q < g->monitors.size(); q++) {
         int nf = 0;
-        if (!rd(fc.f, &nf, sizeof nf) || nf != mn.nfreq) {
-            set_error(FDTD_ERR_ARG, "checkpoint: monitor frequency count %d does not match %d", nf, mn.nfreq);
+        if (!rd(fc.f, &nf, sizeof nf)) goto short_read;
+        if (nf != g->monitors[q].nfreq) {
+            set_error(FDTD_ERR_ARG, "checkpoint: monitor frequency count %d does not match %d", nf,
+                      g->monitors[q].nfreq);
             return false;
         }
-        buf.resize(2 * (size_t)nf * sizeof(double2));
-        if (!rd(fc.f, buf.data(), buf.size())) goto short_read;
-        CK(cudaMemcpy(mn.d_acc, buf.data(), buf.size(), cudaMemcpyHostToDevice));
+        acc[q].resize(2 * (size_t)nf * sizeof(double2));
+        if (!rd(fc.f, acc[q].data(), acc[q].size())) goto short_read;
     }
     {
         const size_t pb = 6 * (size_t)g->nx * g->ny * sizeof(float);
+        std::vector<int> pk(hdr[7]);
+        std::vector<std::vector<char>> pdata(hdr[7]);
         for (int q = 0; q < hdr[7]; q++) {
-            int k = 0;
-            buf.resize(pb);
-            if (!rd(fc.f, &k, sizeof k) || !rd(fc.f, buf.data(), pb)) goto short_read;
-            Plane *pl = grid_plane(g, k, true);
-            if (!pl) return false;
-            CK(cudaMemcpy(pl->p, buf.data(), pb, cudaMemcpyHostToDevice));
+            pdata[q].resize(pb);
+            if (!rd(fc.f, &pk[q], sizeof(int)) || !rd(fc.f, pdata[q].data(), pb)) goto short_read;
+            if (pk[q] < 0 || pk[q] >= g->nz) {
+                set_error(FDTD_ERR_ARG, "checkpoint: source plane z = %d outside the grid", pk[q]);
+                return false;
+            }
         }
         const size_t fb = (size_t)g->n * esize(g);
-        buf.resize(fb);
+        std::vector<std::vector<char>> fields(6);
         for (int m = 0; m < 6; m++) {
-            if (!rd(fc.f, buf.data(), fb)) goto short_read;
-            CK(cudaMemcpy(g->f[g->cur][m], buf.data(), fb, cudaMemcpyHostToDevice));
+            fields[m].resize(fb);
+            if (!rd(fc.f, fields[m].data(), fb)) goto short_read;
         }
+        size_t sz[3] = {0, 0, 0};
+        std::vector<std::vector<char>> psi;
         if (hdr[8]) {
-            size_t sz[3];
             psi_sizes(g, sz);
+            psi.resize(12);
             for (int a = 0; a < 3; a++)
                 for (int w = 0; w < 4; w++) {
-                    buf.resize(sz[a]);
-                    if (!rd(fc.f, buf.data(), sz[a])) goto short_read;
-                    if (!dalloc(&g->psi[g->cur][a][w], sz[a], g->st)) return false;
-                    CK(cudaMemcpy(g->psi[g->cur][a][w], buf.data(), sz[a], cudaMemcpyHostToDevice));
+                    psi[4 * a + w].resize(sz[a]);
+                    if (!rd(fc.f, psi[4 * a + w].data(), sz[a])) goto short_read;
                 }
         }
+        // ---- allocate what the file needs (the only step that can still fail
+        //      before device state changes; new planes and auxiliaries start zero)
+        std::vector<Plane *> pl(hdr[7]);
+        for (int q = 0; q < hdr[7]; q++)
+            if (!(pl[q] = grid_plane(g, pk[q], true))) return false;
+        if (g->boundary == FDTD_BOUNDARY_CPML) {
+            psi_sizes(g, sz);
+            for (int a = 0; a < 3; a++)
+                for (int w = 0; w < 4; w++)
+                    if (!dalloc(&g->psi[g->cur][a][w], sz[a], g->st)) return false;
+        }
+        // ---- write device state, in stream order
+        for (size_t q = 0; q < g->monitors.size(); q++)
+            CK(cudaMemcpyAsync(g->monitors[q].d_acc, acc[q].data(), acc[q].size(), cudaMemcpyHostToDevice, g->st));
+        for (auto &p : g->planes) {
+            int q = 0;
+            while (q < hdr[7] && pl[q] != &p) q++;
+            if (q < hdr[7]) CK(cudaMemcpyAsync(p.p, pdata[q].data(), pb, cudaMemcpyHostToDevice, g->st));
+            else CK(cudaMemsetAsync(p.p, 0, pb, g->st));  // a plane of this grid the saved run did not hold
+        }
+        for (int m = 0; m < 6; m++)
+            CK(cudaMemcpyAsync(g->f[g->cur][m], fields[m].data(), fb, cudaMemcpyHostToDevice, g->st));
+        if (g->boundary == FDTD_BOUNDARY_CPML)
+            for (int a = 0; a < 3; a++)
+                for (int w = 0; w < 4; w++) {
+                    if (hdr[8])
+                        CK(cudaMemcpyAsync(g->psi[g->cur][a][w], psi[4 * a + w].data(), sz[a],
+                                           cudaMemcpyHostToDevice, g->st));
+                    else
+                        CK(cudaMemsetAsync(g->psi[g->cur][a][w], 0, sz[a], g->st));
+                }
+        CK(cudaMemcpyAsync(g->d_step, &steps[1], sizeof(long long), cudaMemcpyHostToDevice, g->st));
+        // host buffers are pageable: wait before they go out of scope
+        CK(cudaStreamSynchronize(g->st));
     }
-    CK(cudaMemcpy(g->d_step, &steps[1], sizeof(long long), cudaMemcpyHostToDevice));
     g->host_steps = steps[0];
     g->fields_from_host = false;
     g->pp_synced = false;

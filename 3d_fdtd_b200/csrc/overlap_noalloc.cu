@@ -16,6 +16,7 @@
 // call overwrites rows [0, ny) before reading them, so nothing needs clearing,
 // but two calls whose kernels overlap on the GPU (different streams, no
 // ordering between them) race on the array and may return wrong sums.
+#include <cstdint>
 #include <mutex>
 
 #include "common.cuh"
@@ -102,6 +103,17 @@ extern "C" int fdtd_mode_overlap_plane_noalloc(const void *ex, const void *ey, c
     if (!ex || !ey || !hx || !hy || !mode_fields || !result || nx <= 0 || ny <= 0 || mode_i <= 0 || mode_j <= 0 ||
         !(ratio > 0) || !(disc > 0) || (precision != FDTD_F64 && precision != FDTD_F32)) {
         set_error(FDTD_ERR_ARG, "fdtd_mode_overlap_plane_noalloc: invalid argument");
+        return FDTD_ERR_ARG;
+    }
+    // the mode and the result are read and written as double2 (16-byte
+    // accesses); a misaligned pointer would fault the kernel and poison the
+    // caller's context, so it is refused here, before any launch
+    const size_t esz = precision == FDTD_F64 ? sizeof(double) : sizeof(float);
+    if (((uintptr_t)mode_fields | (uintptr_t)result) % 16 != 0 ||
+        ((uintptr_t)ex | (uintptr_t)ey | (uintptr_t)hx | (uintptr_t)hy) % esz != 0) {
+        set_error(FDTD_ERR_ARG,
+                  "fdtd_mode_overlap_plane_noalloc: mode_fields and result must be 16-byte aligned and the field "
+                  "planes aligned to their element size");
         return FDTD_ERR_ARG;
     }
     if (ny > kMaxRows) {

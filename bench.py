@@ -137,58 +137,82 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # the reference's own C (CPU baseline and --impl reference)
 # ---------------------------------------------------------------------------
-def reference_throughput(max_seconds: float, min_steps: int, max_steps: int, threads: int) -> dict:
+class ReferenceRun:
     """The reference's step + mode source + two mode overlaps per time step on the
-    same grid (Mur boundary: the reference has no CPML), on `threads` cores."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from bindings import Complex, Reference
-    R = Reference()
-    R.set_threads(threads)
-    nx, ny, nz, dx = W["nx"], W["ny"], W["nz"], W["dx"]
-    dt = 0.99 * dx / math.sqrt(3)
-    tf = R.timefield3d_new(nx, ny, nz, dx)
-    rasterise(R.lib, tf)
-    tmp = tempfile.mkdtemp()
-    modes = []
-    for name in ("c1_in_te0", "c1_out_te0"):
-        txt = os.path.join(tmp, name + ".txt")
-        with gzip.open(os.path.join(MODES, name + ".txt.gz"), "rb") as fi, open(txt, "wb") as fo:
-            shutil.copyfileobj(fi, fo)
-        modes.append(R.load_mode(txt))
-    shutil.rmtree(tmp)
-    amp, phase = source_tables(max_steps + 1, dt)
-    acc = [Complex(), Complex()]
-    n = 0
-    t0 = time.perf_counter()
-    while n < max_steps and (n < min_steps or time.perf_counter() - t0 < max_seconds):
-        R.timefield3d_mode_source(tf, W["cx"], W["cy"], W["src_z"], modes[0], phase[n], amp[n], 0)
-        R.timefield3d_apply_timestep_omp_full(tf, dt)
-        R.timefield3d_mode_overlap(tf, W["cx"], W["cy"], W["launch_z"], modes[0], phase[n], 0, C.byref(acc[0]))
-        R.timefield3d_mode_overlap(tf, W["cx"], W["cy"], W["out_z"], modes[1], phase[n], 0, C.byref(acc[1]))
-        n += 1
-    el = time.perf_counter() - t0
-    R.timefield3d_free(tf)
-    return {"mcells": nx * ny * nz * n / el / 1e6, "steps": n, "seconds": el, "threads": threads}
+    same grid (Mur boundary: the reference has no CPML), on `threads` cores.  The
+    grid and the modes are set up once; `sample(n)` times n further time steps."""
+
+    def __init__(self, threads: int):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from bindings import Complex, Reference
+        self.R = R = Reference()
+        R.set_threads(threads)
+        self.threads = threads
+        nx, ny, nz, dx = W["nx"], W["ny"], W["nz"], W["dx"]
+        self.dt = 0.99 * dx / math.sqrt(3)
+        self.tf = R.timefield3d_new(nx, ny, nz, dx)
+        rasterise(R.lib, self.tf)
+        tmp = tempfile.mkdtemp()
+        self.modes = []
+        for name in ("c1_in_te0", "c1_out_te0"):
+            txt = os.path.join(tmp, name + ".txt")
+            with gzip.open(os.path.join(MODES, name + ".txt.gz"), "rb") as fi, open(txt, "wb") as fo:
+                shutil.copyfileobj(fi, fo)
+            self.modes.append(R.load_mode(txt))
+        shutil.rmtree(tmp)
+        self.amp, self.phase = source_tables(W["time_steps"], self.dt)
+        self.acc = [Complex(), Complex()]
+        self.n = 0
+
+    def sample(self, steps: int) -> dict:
+        R, tf, m = self.R, self.tf, self.modes
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            n = self.n % W["time_steps"]
+            R.timefield3d_mode_source(tf, W["cx"], W["cy"], W["src_z"], m[0], self.phase[n], self.amp[n], 0)
+            R.timefield3d_apply_timestep_omp_full(tf, self.dt)
+            R.timefield3d_mode_overlap(tf, W["cx"], W["cy"], W["launch_z"], m[0], self.phase[n], 0,
+                                       C.byref(self.acc[0]))
+            R.timefield3d_mode_overlap(tf, W["cx"], W["cy"], W["out_z"], m[1], self.phase[n], 0, C.byref(self.acc[1]))
+            self.n += 1
+        el = time.perf_counter() - t0
+        cells = W["nx"] * W["ny"] * W["nz"]
+        return {"mcells": cells * steps / el / 1e6, "steps": steps, "seconds": el, "threads": self.threads}
+
+    def close(self):
+        self.R.timefield3d_free(self.tf)
+
+
+REF_SAMPLE_STEPS = 50      # time steps per bench step of the reference arm
+CPU_BASELINE_STEPS = 150   # time steps of the cpu_baseline leg (about 15 s on 16 cores)
+
+
+def reference_threads() -> int:
+    # the reference's OpenMP z-slabs must hold >= 2 planes each (timefield3d.c:2794-2848)
+    return max(1, min(os.cpu_count() or 1, W["nz"] // 2))
 
 
 def reference_arm(args, rank: int) -> None:
     if rank != 0:
         return
-    threads = max(1, min(os.cpu_count() or 1, W["nz"] // 2))
+    run = ReferenceRun(reference_threads())
+    run.sample(2)   # first touch of the grid's pages
     vals = []
     for s in range(args.warmup + args.steps):
-        r = reference_throughput(1e9, 3, 3, threads)
+        r = run.sample(REF_SAMPLE_STEPS if s >= args.warmup else 5)
         if s >= args.warmup:
             vals.append(r)
+    run.close()
     v = statistics.median([r["mcells"] for r in vals])
-    ms = statistics.median([r["seconds"] / r["steps"] * W["time_steps"] * 1e3 for r in vals])
-    sample = f"3 of {W['time_steps']} time steps per bench step (grid {W['nx']}x{W['ny']}x{W['nz']}, " \
-             "reference Mur boundary, mode source + 2 overlaps per time step), extrapolated"
+    ms = statistics.median([r["seconds"] * 1e3 for r in vals])
+    sample = f"{REF_SAMPLE_STEPS} consecutive of {W['time_steps']} time steps per bench step (grid " \
+             f"{W['nx']}x{W['ny']}x{W['nz']}, reference Mur boundary, mode source + 2 overlaps per time step, " \
+             "FP64 as the reference computes); ms_per_step is that sample's wall time"
     line = {"impl": "reference", "metric": "Yee Mcell-updates/s", "value": v, "unit": "Mcell-updates/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": config_block(args),
-            "cpu_baseline": {"value": v, "unit": "Mcell-updates/s", "cores": threads, "kind": "reference",
+            "cpu_baseline": {"value": v, "unit": "Mcell-updates/s", "cores": run.threads, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": v, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -209,12 +233,12 @@ def config_block(args) -> dict:
 class Taper:
     """One simulation of the workload on one GPU."""
 
-    def __init__(self, fd, time_steps: int, variant: int = 0):
+    def __init__(self, fd, time_steps: int, variant: int = 0, precision: int | None = None):
         self.fd, self.T = fd, time_steps
         lib = fd.lib
         nx, ny, nz, dx = W["nx"], W["ny"], W["nz"], W["dx"]
         self.dt = 0.99 * dx / math.sqrt(3)
-        self.grid = fd.Grid(nx, ny, nz, dx, fd.F32)
+        self.grid = fd.Grid(nx, ny, nz, dx, fd.F32 if precision is None else precision)
         self.t = self.grid.t
         rasterise(lib, self.t)
         fd.call("timefield3d_set_cpml", self.t, W["cpml"], 3, -1.0, 1.0, 0.0)
@@ -250,13 +274,21 @@ class Taper:
         self.fd.lib.timefield3d_zero_fields(self.t)
         self.fd.call("timefield3d_run", self.t, self.dt, self.T)
 
-    def transmission(self):
+    def amplitude_ratio(self):
+        """t(lambda) = O_out / O_in, the complex ratio the reference driver prints
+        the magnitude of (3d_fdtd.c:139-142)."""
         a, b = (self.fd.Complex * len(self.omega))(), (self.fd.Complex * len(self.omega))()
         self.fd.call("timefield3d_read_overlap_monitor", self.t, self.mon_in, a)
         self.fd.call("timefield3d_read_overlap_monitor", self.t, self.mon_out, b)
         oi = np.array([complex(x.re, x.im) for x in a])
         oo = np.array([complex(x.re, x.im) for x in b])
-        return np.abs(oo / oi) ** 2
+        return oo / oi
+
+    def transmission(self):
+        return np.abs(self.amplitude_ratio()) ** 2
+
+    def close(self):
+        self.grid.close()
 
     def e2e_step(self):
         """Design evaluation through the public API: re-rasterise, upload, run, read."""
@@ -347,14 +379,29 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = world * cells * args.time_steps * args.steps / e2e_s / 1e6
+    # FP32 against FP64: the same workload once on the engine's FP64 path (bit-exact
+    # to the CPU restatement on CPML grids), outside every timed region
+    t32 = sim.amplitude_ratio()
+    f64_check = None
+    if not args.no_f64_check:
+        ref64 = Taper(fd, args.time_steps, 0, fd.F64)
+        ref64.run()
+        t64 = ref64.amplitude_ratio()
+        ref64.close()
+        rel = np.abs(t32 - t64) / np.abs(t64)
+        f64_check = {"rel_err_vs_f64": float(rel.max()), "per_lambda": [float(x) for x in rel],
+                     "tolerance": 1e-3, "quantity": "complex t = O_out/O_in per wavelength"}
     # CPU baseline: the reference on this host's cores (rank 0, N = 1 only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = max(1, min(os.cpu_count() or 1, W["nz"] // 2))
-        r = reference_throughput(args.cpu_seconds, 3, 200, threads)
-        cpu = {"value": r["mcells"], "unit": "Mcell-updates/s", "cores": threads, "kind": "reference",
-               "sample": f"{r['steps']} of {W['time_steps']} time steps of the same grid in {r['seconds']:.1f} s "
-                         "(reference step with its Mur boundary, mode source and 2 overlaps per time step)"}
+        run = ReferenceRun(reference_threads())
+        run.sample(2)
+        r = run.sample(CPU_BASELINE_STEPS)
+        run.close()
+        cpu = {"value": r["mcells"], "unit": "Mcell-updates/s", "cores": r["threads"], "kind": "reference",
+               "sample": f"{r['steps']} consecutive of {W['time_steps']} time steps of the same grid in "
+                         f"{r['seconds']:.1f} s (reference step with its Mur boundary, mode source and 2 overlaps "
+                         "per time step, FP64)"}
     if rank == 0:
         line = {"metric": "Yee Mcell-updates/s", "value": value, "unit": "Mcell-updates/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -374,7 +421,8 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
                         "d2h_bytes_per_step": sim.d2h_bytes()},
                 "gpu_launches": launches, "clocks": clk,
                 "transmission": {"lambda_um": W["lams"], "T": [round(float(x), 6) for x in trans],
-                                 "T_e2e_equal": bool(np.allclose(trans, trans_e2e, rtol=1e-6))}}
+                                 "T_e2e_equal": bool(np.allclose(trans, trans_e2e, rtol=1e-6)),
+                                 **(f64_check or {})}}
         print(json.dumps(line), flush=True)
     ranks.close()
 
@@ -388,6 +436,7 @@ def main():
     ap.add_argument("--time-steps", type=int, default=W["time_steps"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-f64-check", action="store_true", help="skip the FP64 run that checks the FP32 transmission")
     ap.add_argument("--yee-variant", choices=["auto", "flat", "flat4", "fused", "wave"], default="auto")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))

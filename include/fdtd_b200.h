@@ -438,7 +438,10 @@ int timefield3d_read_kernel_timing(timefield3d psi, double *total_ms, long long 
  * z-plane (x fastest; double for FDTD_F64, float for FDTD_F32), mode_fields
  * to the 6*mode_i*mode_j complex values of a power-normalised mode in the
  * layout of mode.fields.m, result to one complex that receives
- * -disc^2/2 * sum; ratio = disc / mode disc.  Work is queued on `stream`
+ * -disc^2/2 * sum; ratio = disc / mode disc.  mode_fields and result must
+ * be 16-byte aligned (cudaMalloc'd memory is) and ex..hy aligned to their
+ * element size; other pointers are refused with FDTD_ERR_ARG before any
+ * launch.  Work is queued on `stream`
  * (a cudaStream_t, or NULL for the default stream); the call returns at once.
  * Scratch is a fixed file-scope device array of one partial per plane row:
  * ny may be at most 8192 (larger planes are rejected with FDTD_ERR_ARG).  The

@@ -96,3 +96,66 @@ def test_runs_are_deterministic(fd, gpu):
         fd.call("timefield3d_run", g.t, dt, 160)
         out.append((g.fields(), monitor(fd, g, mon)))
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.gpu
+def test_truncated_checkpoint_leaves_grid_unchanged(fd, gpu, tmp_path):
+    # a file cut inside the field data: the load is refused and nothing of the
+    # grid (fields, monitors, step count) changes
+    T = 120
+    ck = tmp_path / "full.ckpt"
+    a, mon_a, dt = setup(fd, T)
+    fd.call("timefield3d_run", a.t, dt, 64)
+    fd.call("timefield3d_checkpoint_save", a.t, str(ck).encode())
+    raw = ck.read_bytes()
+    field_bytes = 6 * a.nx * a.ny * a.nz * 4
+    cut = tmp_path / "cut.ckpt"
+    cut.write_bytes(raw[: len(raw) - field_bytes // 2 - 12 * 4096])
+    b, mon_b, _ = setup(fd, T)
+    fd.call("timefield3d_run", b.t, dt, 24)
+    before = (b.fields(), monitor(fd, b, mon_b), fd.lib.timefield3d_step_count(b.t))
+    assert fd.lib.timefield3d_checkpoint_load(b.t, str(cut).encode()) == fd.FDTD_ERR_ARG
+    assert b"truncated" in fd.lib.fdtd_last_error_message()
+    fd.lib.fdtd_clear_error()
+    after = (b.fields(), monitor(fd, b, mon_b), fd.lib.timefield3d_step_count(b.t))
+    assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
+    assert before[2] == after[2] == 24
+
+
+@pytest.mark.gpu
+def test_load_into_grid_that_already_ran(fd, gpu, tmp_path):
+    # the target grid has run other steps first (its CPML auxiliaries, source
+    # plane and monitors hold other values); after the load it continues
+    # exactly like the saved run
+    T = 160
+    ck = str(tmp_path / "run.ckpt").encode()
+    a, mon_a, dt = setup(fd, T)
+    fd.call("timefield3d_run", a.t, dt, 80)
+    fd.call("timefield3d_checkpoint_save", a.t, ck)
+    fd.call("timefield3d_run", a.t, dt, T - 80)
+    b, mon_b, _ = setup(fd, T)
+    fd.call("timefield3d_run", b.t, dt, 131)
+    fd.call("timefield3d_checkpoint_load", b.t, ck)
+    assert fd.lib.timefield3d_step_count(b.t) == 80
+    fd.call("timefield3d_run", b.t, dt, T - 80)
+    assert np.array_equal(monitor(fd, a, mon_a), monitor(fd, b, mon_b))
+    assert np.array_equal(a.fields(), b.fields())
+
+
+@pytest.mark.gpu
+def test_load_without_cpml_state_zeroes_auxiliaries(fd, gpu, tmp_path):
+    # a checkpoint of a grid that had not stepped yet holds no CPML auxiliaries;
+    # loading it into a grid that ran must leave that grid's auxiliaries zero,
+    # so the run equals one from a fresh grid
+    T = 100
+    ck = str(tmp_path / "fresh.ckpt").encode()
+    a, mon_a, dt = setup(fd, T)
+    fd.call("timefield3d_checkpoint_save", a.t, ck)
+    fd.call("timefield3d_run", a.t, dt, T)
+    b, mon_b, _ = setup(fd, T)
+    fd.call("timefield3d_run", b.t, dt, 77)
+    fd.call("timefield3d_checkpoint_load", b.t, ck)
+    assert fd.lib.timefield3d_step_count(b.t) == 0
+    fd.call("timefield3d_run", b.t, dt, T)
+    assert np.array_equal(monitor(fd, a, mon_a), monitor(fd, b, mon_b))
+    assert np.array_equal(a.fields(), b.fields())

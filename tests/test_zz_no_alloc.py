@@ -23,13 +23,16 @@ pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
-def test_noalloc_overlap_matches_regular_entry_point(fd, gpu):
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_noalloc_overlap_matches_regular_entry_point(fd, gpu, prec):
     import torch
+    precision = fd.F64 if prec == "f64" else fd.F32
+    np_dtype = np.float64 if prec == "f64" else np.float32
     p = wg_setup()
     nx, ny, nz, dx = p["nx"], p["ny"], p["nz"], p["dx"]
     dt = 0.99 * dx / math.sqrt(3)
     omega = 2 * fd.REF_PI / p["lam"]
-    grid = fd.Grid(nx, ny, nz, dx, fd.F64)
+    grid = fd.Grid(nx, ny, nz, dx, precision)
     wg_geometry(fd.lib, grid.t, p, None, None)
     mode = fd.read_mode_file(os.path.join(GOLDEN, "modes", "small_te0.txt.gz"))
     b, t = p["core"]
@@ -49,10 +52,12 @@ def test_noalloc_overlap_matches_regular_entry_point(fd, gpu):
         acc = fd.Complex()
         ref = fd.lib.timefield3d_mode_overlap(grid.t, cx, cy, z, mode.struct, 0.0, rev, C.byref(acc))
         fd.check("timefield3d_mode_overlap")
-        planes = [torch.from_numpy(np.ascontiguousarray(f[z, :, :, m])).to(dev) for m in (0, 1, 3, 4)]
+        # the FP32 grid's host mirror holds its float values exactly
+        planes = [torch.from_numpy(np.ascontiguousarray(f[z, :, :, m].astype(np_dtype))).to(dev)
+                  for m in (0, 1, 3, 4)]
         md = torch.from_numpy(mode.fields.copy()).to(dev)      # normalised in place by the call above
         rc = fd.lib.fdtd_mode_overlap_plane_noalloc(
-            planes[0].data_ptr(), planes[1].data_ptr(), planes[2].data_ptr(), planes[3].data_ptr(), fd.F64,
+            planes[0].data_ptr(), planes[1].data_ptr(), planes[2].data_ptr(), planes[3].data_ptr(), precision,
             nx, ny, cx, cy, md.data_ptr(), mode.mi, mode.mj, dx / mode.disc, rev, dx, result.data_ptr(),
             stream.cuda_stream)
         assert rc == fd.FDTD_OK, fd.lib.fdtd_last_error_message()
@@ -70,3 +75,21 @@ def test_noalloc_overlap_rejects_oversized_plane(fd, gpu):
     assert rc == fd.FDTD_ERR_ARG
     assert "8192" in fd.lib.fdtd_last_error_message().decode()
     fd.lib.fdtd_clear_error()
+
+
+def test_noalloc_overlap_rejects_misaligned_pointers(fd, gpu):
+    # refused on the host before any launch: result / mode must be 16-byte aligned,
+    # field planes aligned to their element size (nothing is dereferenced)
+    ok16, off8, off4 = C.c_void_p(256), C.c_void_p(264), C.c_void_p(260)
+    cases = [
+        (ok16, ok16, fd.F64, off8),   # result at 8 bytes past a 16-byte boundary
+        (ok16, off8, fd.F64, ok16),   # mode_fields likewise
+        (off4, ok16, fd.F64, ok16),   # a double plane at 4 bytes
+        (C.c_void_p(258), ok16, fd.F32, ok16),   # a float plane at 2 bytes
+    ]
+    for plane, mode_ptr, prec, result in cases:
+        rc = fd.lib.fdtd_mode_overlap_plane_noalloc(plane, ok16, ok16, ok16, prec, 4, 4, 2, 2, mode_ptr, 2, 2,
+                                                    1.0, 0, 0.05, result, None)
+        assert rc == fd.FDTD_ERR_ARG
+        assert "aligned" in fd.lib.fdtd_last_error_message().decode()
+        fd.lib.fdtd_clear_error()

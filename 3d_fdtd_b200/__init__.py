@@ -25,7 +25,7 @@ FDTD_OK, FDTD_ERR_NO_DEVICE, FDTD_ERR_CUDA, FDTD_ERR_ARG, FDTD_ERR_ALLOC = 0, 1,
 FDTD_ERR_UNSUPPORTED, FDTD_ERR_TIMEOUT, FDTD_ERR_NONFINITE = 5, 6, 7
 F64, F32 = 0, 1
 MUR, CPML, PEC = 0, 1, 2
-YEE_AUTO, YEE_FLAT, YEE_FUSED, YEE_FLAT4, YEE_WAVE = 0, 1, 2, 3, 4
+YEE_AUTO, YEE_FLAT, YEE_FUSED, YEE_FLAT4, YEE_WAVE, YEE_STREAM = 0, 1, 2, 3, 4, 5
 
 # the reference's constants (3d_fdtd.c:12, timefield3d.c:3)
 REF_PI = 3.141592652
@@ -187,6 +187,7 @@ SIGNATURES = {
     "timefield3d_set_wave_steps": (i, [T, i, i, i]),
     "fdtd_wave_schedule": (i, [i, i, i, i, i, i, i, ip, i, i, ip, i, ip]),
     "timefield3d_read_kernel_timing": (i, [T, dp, C.POINTER(ll)]),
+    "fdtd_stream_plan": (i, [i, i, i, i, i, i, ip, i, ip, ip, C.POINTER(C.c_longlong)]),
     "fdtd_mode_overlap_plane_noalloc": (i, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, i, i, i, i, i,
                                             C.c_void_p, i, i, d, i, d, C.c_void_p, C.c_void_p]),
 }

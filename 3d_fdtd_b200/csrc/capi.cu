@@ -797,11 +797,12 @@ int timefield3d_set_yee_variant(timefield3d psi, int variant)
     LOCK;
     Grid *g = grid_lookup(psi);
     if (!g) return FDTD_ERR_ARG;
-    if (variant < FDTD_YEE_AUTO || variant > FDTD_YEE_WAVE) {
+    if (variant < FDTD_YEE_AUTO || variant > FDTD_YEE_STREAM) {
         set_error(FDTD_ERR_ARG, "yee variant %d", variant);
         return FDTD_ERR_ARG;
     }
     g->yee_variant = variant;
+    g->pp_synced = false;   // a ping-pong design starts again from two equal sets
     g->version++;
     return FDTD_OK;
 }

@@ -366,6 +366,7 @@ Grid::~Grid()
         dfree(d_err);
         delete fmaps[0];
         delete fmaps[1];
+        dfree(d_tiles);
         dfree(d_flag);
         for (auto &mn : monitors) { dfree(mn.d_omega); dfree(mn.d_acc); priv_mode_free(mn.mode_key); }
         dfree(d_probes); dfree(d_probe_buf); dfree(d_probe_count);
@@ -665,11 +666,49 @@ static bool fast32_path(const Grid *g)
     return g->prec == FDTD_F32 && g->boundary != FDTD_BOUNDARY_MUR && !g->sig_m && !g->mu_nonunit;
 }
 
-// which kernel design the fast path uses: the flat pair by default (it runs
-// at a higher fraction of HBM bandwidth on B200 than the plane-streaming kernel)
+// which kernel design the fast path uses: the one-pass streaming kernel where
+// the grid allows it (FDTD_YEE_STREAM, and opt-in until measured), the
+// plane-streaming TMA / cp.async kernel on request, else the flat pair
+static bool stream_path(const Grid *g)
+{
+    return fast32_path(g) && g->yee_variant == FDTD_YEE_STREAM && stream_supported(g->nx, g->ny, g->nz, g->sig_e);
+}
+
 static bool fused_path(const Grid *g)
 {
     return fast32_path(g) && g->yee_variant == FDTD_YEE_FUSED && fused_supported(g->nx, g->ny, g->nz);
+}
+
+// designs that read one field set and write the other
+static bool pingpong_path(const Grid *g) { return stream_path(g) || fused_path(g); }
+
+// tile plan of the streaming kernel for the grid's shape (rebuilt when the
+// shape, CPML thickness, loss or device changes)
+static bool stream_prepare(Grid *g)
+{
+    int dev = 0, nsm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int L = g->boundary == FDTD_BOUNDARY_CPML ? g->L : 0;
+    const int key[6] = {g->nx, g->ny, g->nz, L, g->sig_e ? 1 : 0, nsm};
+    if (g->d_tiles && std::equal(key, key + 6, g->splan_key)) return true;
+    StreamPlan p;
+    if (!stream_plan(g->nx, g->ny, g->nz, L, g->sig_e, nsm, &p)) {
+        set_error(FDTD_ERR_UNSUPPORTED, "streaming Yee kernel: no tile plan for grid %dx%dx%d", g->nx, g->ny, g->nz);
+        return false;
+    }
+    if (!stream_configure(p.smem)) {
+        set_error(FDTD_ERR_CUDA, "streaming Yee kernel: %zu bytes of shared memory per block refused", p.smem);
+        return false;
+    }
+    CK(cudaStreamSynchronize(g->st));
+    dfree(g->d_tiles);
+    if (!dalloc(&g->d_tiles, p.tiles.size() * sizeof(StreamTile), g->st, false)) return false;
+    CK(cudaMemcpyAsync(g->d_tiles, p.tiles.data(), p.tiles.size() * sizeof(StreamTile), cudaMemcpyHostToDevice, g->st));
+    g->splan = std::move(p);
+    std::copy(key, key + 6, g->splan_key);
+    g->version++;
+    return true;
 }
 
 // FP32 E-update coefficients of the fused path: cb = main/dx, ca = main*coef,
@@ -691,7 +730,7 @@ bool grid_prepare_step(Grid *g, double dt)
         set_error(FDTD_ERR_ARG, "delta_t must be positive and finite (got %g)", dt);
         return false;
     }
-    const bool fused = fused_path(g);
+    const bool fused = pingpong_path(g);
     if (g->boundary == FDTD_BOUNDARY_MUR) {
         size_t bytes = (size_t)g->n * esize(g);
         for (int m = 0; m < 6; m++)
@@ -754,8 +793,9 @@ bool grid_prepare_step(Grid *g, double dt)
             g->fmaps[0] = g->fmaps[1] = nullptr;
             g->version++;
         }
+        if (stream_path(g) && !stream_prepare(g)) return false;
         // TMA descriptors of the fused kernel (host-side encode; they only depend on the buffers)
-        if (fused && !g->fmaps[0] && fused_tma_supported(g->nx, g->ny, g->nz)) {
+        if (fused_path(g) && !g->fmaps[0] && fused_tma_supported(g->nx, g->ny, g->nz)) {
             {
                 for (int s = 0; s < 2; s++) {
                     FusedMaps *m = new FusedMaps();
@@ -917,6 +957,32 @@ static bool step_fused(Grid *g, double dt)
     return true;
 }
 
+static bool step_stream(Grid *g, double dt)
+{
+    StreamArgs a{};
+    a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
+    a.L = g->boundary == FDTD_BOUNDARY_CPML ? g->L : 0;
+    a.ty = g->splan.ty;
+    const int in = g->cur, out = 1 - g->cur;
+    for (int m = 0; m < 6; m++) { a.f_in[m] = (const float *)g->f[in][m]; a.f_out[m] = (float *)g->f[out][m]; }
+    for (int c = 0; c < 3; c++) { a.cb[c] = g->cb[c]; a.ca[c] = g->sig_e ? g->ca[c] : nullptr; }
+    a.hb = (float)(dt / g->dx);
+    a.dx = (float)g->dx;
+    for (int ax = 0; ax < 3; ax++) {
+        for (int w = 0; w < 4; w++) {
+            a.psi_in[ax][w] = (const float *)g->psi[in][ax][w];
+            a.psi_out[ax][w] = (float *)g->psi[out][ax][w];
+        }
+        for (int w = 0; w < 6; w++) a.prof[w][ax] = (const float *)g->prof[w][ax];
+    }
+    a.src = source_table(g);
+    a.tiles = g->d_tiles;
+    launch_yee_stream(a, g->splan, g->st);
+    CKL("streaming step");
+    g->cur = out;
+    return true;
+}
+
 static bool schedule_job(Grid *g, SourceJob *sj);
 
 bool enqueue_after_step(Grid *g, double dt)
@@ -1034,6 +1100,7 @@ bool enqueue_step(Grid *g, double dt, bool with_extras)
     // read after a replay (a plain record during capture is only a dependency)
     if (g->cap_ev) CK(cudaEventRecordWithFlags(g->cap_ev[2 * g->cap_step], g->st, cudaEventRecordExternal));
     if (g->prec == FDTD_F64) ok = step_split<double>(g, dt);
+    else if (stream_path(g)) ok = step_stream(g, dt);
     else if (fused_path(g)) ok = step_fused(g, dt);
     else if (fast32_path(g)) ok = step_flat(g, dt);
     else ok = step_split<float>(g, dt);

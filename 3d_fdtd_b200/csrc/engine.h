@@ -122,6 +122,10 @@ struct Grid {
     double coef_dt = 0;
     bool coef_valid = false;
     FusedMaps *fmaps[2] = {};        // TMA descriptors with set s as input (null: cp.async kernel)
+    // one-pass streaming step (yee_stream.cu): tile plan of this grid's shape
+    StreamPlan splan;
+    StreamTile *d_tiles = nullptr;
+    int splan_key[6] = {-1, -1, -1, -1, -1, -1};   // nx ny nz L lossy nsm the plan was built for
     int *d_err = nullptr;            // device error flag (a bounded wait gave up)
     int *h_err = nullptr;            // pinned
 

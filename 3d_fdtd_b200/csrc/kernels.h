@@ -184,6 +184,39 @@ Plan4 flat4_plan(const FlatArgs &a);
 // and the shell on `side` (fork/join through the two events) for each field.
 void launch_flat4_step(const FlatArgs &a, cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join);
 
+// yee_stream.cu: the FP32 step in one pass (E and H of every cell), z-planes
+// streamed through shared memory by (band of rows, chunk of planes) tiles
+struct StreamTile {
+    int j0, rows;            // owned rows [j0, j0 + rows), all in 1..ny-2
+    int k0, k1;              // owned planes [k0, k1), all in 1..nz-2
+};
+struct StreamPlan {
+    int ty = 0;              // rows of the largest band (shared memory holds ty + 1 rows)
+    int threads = 0;         // block size: (ty + 1) rows of nx/4 threads, rounded up to a warp
+    size_t smem = 0;         // dynamic shared memory per block (bytes)
+    std::vector<StreamTile> tiles;   // one block each, all resident at once
+};
+struct StreamArgs {
+    int nx, ny, nz, L, ty;
+    const float *f_in[6];
+    float *f_out[6];
+    const float *cb[3];
+    const float *ca[3];      // null: lossless
+    float hb, dx;
+    const float *psi_in[3][4];
+    float *psi_out[3][4];
+    const float *prof[6][3];
+    SourcePlanes src;
+    const StreamTile *tiles;
+};
+constexpr size_t kStreamSmemBudget = 232448;   // dynamic shared memory per block, sm_100 maximum
+int stream_supported(int nx, int ny, int nz, bool lossy);
+// tiles for a grid on a device with nsm SMs; false when the grid cannot use the kernel
+bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan *out);
+// allow `smem` bytes of dynamic shared memory for every instantiation (host, not stream-ordered)
+bool stream_configure(size_t smem);
+void launch_yee_stream(const StreamArgs &a, const StreamPlan &p, cudaStream_t st);
+
 // yee_wave.cu: S steps of the flat4 update in one persistent, cooperative
 // launch, wavefront-ordered in z (see the file's header)
 struct WaveItem {

@@ -326,7 +326,7 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
     ranks = importlib.import_module("3d_fdtd_b200.replicas").Ranks("nccl", timeout_s=120)
     barrier, max_over_ranks = ranks.barrier, ranks.max
 
-    sim = Taper(fd, args.time_steps, {"auto": 0, "flat": 1, "fused": 2, "flat4": 3, "wave": 4}[args.yee_variant])
+    sim = Taper(fd, args.time_steps, {"auto": 0, "flat": 1, "fused": 2, "flat4": 3, "wave": 4, "stream": 5}[args.yee_variant])
     stream = torch.cuda.ExternalStream(fd.lib.timefield3d_get_stream(sim.t))
     cells = W["nx"] * W["ny"] * W["nz"]
     # warm-up: full runs (graph capture, clocks)
@@ -437,7 +437,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-f64-check", action="store_true", help="skip the FP64 run that checks the FP32 transmission")
-    ap.add_argument("--yee-variant", choices=["auto", "flat", "flat4", "fused", "wave"], default="auto")
+    ap.add_argument("--yee-variant", choices=["auto", "flat", "flat4", "fused", "wave", "stream"], default="auto")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -231,7 +231,8 @@ enum fdtd_precision { FDTD_F64 = 0, FDTD_F32 = 1 };
  * AUTO picks flat4 where nx allows, else flat.  wave's fields are
  * bit-identical to flat4's. */
 enum fdtd_yee_variant {
-    FDTD_YEE_AUTO = 0, FDTD_YEE_FLAT = 1, FDTD_YEE_FUSED = 2, FDTD_YEE_FLAT4 = 3, FDTD_YEE_WAVE = 4
+    FDTD_YEE_AUTO = 0, FDTD_YEE_FLAT = 1, FDTD_YEE_FUSED = 2, FDTD_YEE_FLAT4 = 3, FDTD_YEE_WAVE = 4,
+    FDTD_YEE_STREAM = 5
 };
 enum fdtd_boundary { FDTD_BOUNDARY_MUR = 0, FDTD_BOUNDARY_CPML = 1, FDTD_BOUNDARY_PEC = 2 };
 
@@ -267,6 +268,16 @@ int timefield3d_set_wave_steps(timefield3d psi, int steps_per_launch, int steps_
  * and the ticket total, or -1 on invalid input. */
 int fdtd_wave_schedule(int nx, int ny, int nz, int cpml_cells, int steps, int sweep, int blocks_per_ticket,
                        const int *job_z, int njobs, int nparts, int *out, int cap, int *tickets);
+/* The tile plan of the FDTD_YEE_STREAM kernel (host computation, no device
+ * work), for inspection and tests.  No reference counterpart.  Grid
+ * nx x ny x nz, CPML thickness (0: none), lossy != 0 when the E update has
+ * loss coefficients, nsm streaming multiprocessors.  Writes 4 ints per tile
+ * into tiles (capacity cap tiles; null to count): first owned row, owned rows,
+ * first owned plane, one past the last owned plane; and the block's row
+ * capacity, threads and dynamic shared memory.  Returns the tile count, or -1
+ * when the grid cannot use the kernel or on invalid input. */
+int fdtd_stream_plan(int nx, int ny, int nz, int cpml_cells, int lossy, int nsm, int *tiles, int cap, int *ty,
+                     int *threads, long long *smem_bytes);
 /* CPML of `thickness` cells on every face, polynomial grading `order`;
  * sigma_max <= 0 selects 0.8 (order+1)/disc; kappa_max >= 1; alpha_max >= 0.
  * Profiles depend on delta_t and are rebuilt when the step size changes.

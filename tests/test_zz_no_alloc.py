@@ -79,7 +79,10 @@ def test_noalloc_overlap_rejects_oversized_plane(fd, gpu):
 
 def test_noalloc_overlap_rejects_misaligned_pointers(fd, gpu):
     # refused on the host before any launch: result / mode must be 16-byte aligned,
-    # field planes aligned to their element size (nothing is dereferenced)
+    # field planes aligned to their element size (nothing is dereferenced).  The
+    # plane is also taller than the scratch allows, so a library without the
+    # alignment check would still refuse the call (for the row count) rather
+    # than launch on these addresses.
     ok16, off8, off4 = C.c_void_p(256), C.c_void_p(264), C.c_void_p(260)
     cases = [
         (ok16, ok16, fd.F64, off8),   # result at 8 bytes past a 16-byte boundary
@@ -88,7 +91,7 @@ def test_noalloc_overlap_rejects_misaligned_pointers(fd, gpu):
         (C.c_void_p(258), ok16, fd.F32, ok16),   # a float plane at 2 bytes
     ]
     for plane, mode_ptr, prec, result in cases:
-        rc = fd.lib.fdtd_mode_overlap_plane_noalloc(plane, ok16, ok16, ok16, prec, 4, 4, 2, 2, mode_ptr, 2, 2,
+        rc = fd.lib.fdtd_mode_overlap_plane_noalloc(plane, ok16, ok16, ok16, prec, 4, 9000, 2, 2, mode_ptr, 2, 2,
                                                     1.0, 0, 0.05, result, None)
         assert rc == fd.FDTD_ERR_ARG
         assert "aligned" in fd.lib.fdtd_last_error_message().decode()

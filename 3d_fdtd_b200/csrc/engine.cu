@@ -671,7 +671,8 @@ static bool fast32_path(const Grid *g)
 // plane-streaming TMA / cp.async kernel on request, else the flat pair
 static bool stream_path(const Grid *g)
 {
-    return fast32_path(g) && g->yee_variant == FDTD_YEE_STREAM && stream_supported(g->nx, g->ny, g->nz, g->sig_e);
+    return fast32_path(g) && g->yee_variant == FDTD_YEE_STREAM &&
+           stream_supported(g->nx, g->ny, g->nz, g->sig_e, g->boundary == FDTD_BOUNDARY_CPML ? g->L : 0);
 }
 
 static bool fused_path(const Grid *g)

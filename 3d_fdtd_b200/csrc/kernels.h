@@ -210,7 +210,9 @@ struct StreamArgs {
     const StreamTile *tiles;
 };
 constexpr size_t kStreamSmemBudget = 232448;   // dynamic shared memory per block, sm_100 maximum
-int stream_supported(int nx, int ny, int nz, bool lossy);
+// staged x-slab auxiliaries per row: 2L, padded to 16 bytes
+__host__ __device__ inline int stream_xpsi_stride(int L) { return (2 * L + 3) & ~3; }
+int stream_supported(int nx, int ny, int nz, bool lossy, int L);
 // tiles for a grid on a device with nsm SMs; false when the grid cannot use the kernel
 bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan *out);
 // allow `smem` bytes of dynamic shared memory for every instantiation (host, not stream-ordered)

@@ -77,11 +77,12 @@ __device__ __forceinline__ void sts4(float *p, const Vf<4> &x)
     *reinterpret_cast<float4 *>(p) = make_float4(x.v[0], x.v[1], x.v[2], x.v[3]);
 }
 
-// ---- CPML state of one quad for one field (E: A0 = 0, H: A0 = 2), read from
-//      the `in` auxiliaries; the 1-D profiles are read where they are used
-//      (a few hundred floats, cached)
+// ---- CPML auxiliaries of one quad for one field (E: A0 = 0, H: A0 = 2).
+//      x-slab: per element, staged in shared memory with the plane (rows of
+//      2L values); y- and z-slab: contiguous in x, read from global memory.
+//      The 1-D profiles are read where they are used (a few hundred floats,
+//      cached).
 struct XPsi {
-    bool any;
     bool valid[4];
     float p0[4], p1[4];
 };
@@ -90,21 +91,27 @@ struct YZPsi {
     Vf<4> pxy, pzy, pxz, pyz;   // as YZSlab: (x,y) (z,y) (x,z) (y,z) for E, alike for H
 };
 
-template <int A0>
-__device__ __forceinline__ void stream_psi_load(XPsi &xs, YZPsi &s, const StreamArgs &a, int q, int j, int k,
-                                                long long ij0, long long nxy)
+// x-slab auxiliaries of the quad from a staged row pair (row0, row1: the two
+// auxiliaries of this field for the cell row)
+__device__ __forceinline__ void stream_xpsi(XPsi &xs, const float *row0, const float *row1, int nx, int L, int q)
 {
-    const int nx = a.nx, L = a.L, i0 = 4 * q;
-    xs.any = i0 < L || i0 + 3 >= nx - L;
-    const long long s0 = 2LL * L * (j + (long long)a.ny * k);
+    const int i0 = 4 * q;
+    const bool any = i0 < L || i0 + 3 >= nx - L;
 #pragma unroll
     for (int e = 0; e < 4; e++) {
         const int i = i0 + e;
         const int si = slab_local(i, nx, L);
-        xs.valid[e] = xs.any && si >= 0 && i >= 1 && i <= nx - 2;
-        xs.p0[e] = xs.valid[e] ? __ldg(a.psi_in[0][A0] + s0 + si) : 0.f;
-        xs.p1[e] = xs.valid[e] ? __ldg(a.psi_in[0][A0 + 1] + s0 + si) : 0.f;
+        xs.valid[e] = any && si >= 0 && i >= 1 && i <= nx - 2;
+        xs.p0[e] = xs.valid[e] ? row0[si] : 0.f;
+        xs.p1[e] = xs.valid[e] ? row1[si] : 0.f;
     }
+}
+
+template <int A0>
+__device__ __forceinline__ void stream_yzpsi_load(YZPsi &s, const StreamArgs &a, int q, int j, int k, long long ij0,
+                                                  long long nxy)
+{
+    const int nx = a.nx, L = a.L, i0 = 4 * q;
     s.sj = slab_local(j, a.ny, L);
     s.sk = slab_local(k, a.nz, L);
     s.pxy = fillv<4>(0.f); s.pzy = s.pxy; s.pxz = s.pxy; s.pyz = s.pxy;
@@ -125,15 +132,13 @@ __device__ __forceinline__ void stream_psi_store(const XPsi &xs, const YZPsi &s,
                                                  int k, long long ij0, long long nxy)
 {
     const int nx = a.nx, L = a.L, i0 = 4 * q;
-    if (xs.any) {
-        const long long s0 = 2LL * L * (j + (long long)a.ny * k);
+    const long long s0 = 2LL * L * (j + (long long)a.ny * k);
 #pragma unroll
-        for (int e = 0; e < 4; e++) {
-            if (!xs.valid[e]) continue;
-            const long long sidx = s0 + slab_local(i0 + e, nx, L);
-            a.psi_out[0][A0][sidx] = xs.p0[e];
-            a.psi_out[0][A0 + 1][sidx] = xs.p1[e];
-        }
+    for (int e = 0; e < 4; e++) {
+        if (!xs.valid[e]) continue;
+        const long long sidx = s0 + slab_local(i0 + e, nx, L);
+        a.psi_out[0][A0][sidx] = xs.p0[e];
+        a.psi_out[0][A0 + 1][sidx] = xs.p1[e];
     }
     if (s.sj >= 0) {
         const long long sy = (long long)i0 + (long long)nx * (s.sj + 2LL * L * k);
@@ -188,8 +193,15 @@ __device__ __forceinline__ Curl3 stream_cpml_curl(XPsi &xs, YZPsi &s, const Stre
     return c;
 }
 
+// 4-byte asynchronous copy (x-slab auxiliary rows when 2L is not a multiple of 4)
+__device__ __forceinline__ void cp_async4(float *smem, const float *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
 template <bool CPML, bool LOSSY>
-__global__ void __launch_bounds__(kStreamMaxThreads, 1) k_yee_stream(StreamArgs a)
+__global__ void __maxnreg__(152) k_yee_stream(StreamArgs a)
 {
     // programmatic dependent launch, as the flat kernels (see k_flat4_merged)
     asm volatile("griddepcontrol.wait;" ::: "memory");
@@ -198,8 +210,9 @@ __global__ void __launch_bounds__(kStreamMaxThreads, 1) k_yee_stream(StreamArgs 
     constexpr int NA = LOSSY ? 12 : 9;   // staged arrays: Hx Hy Hz, Ex Ey Ez, cb0..2 (, ca0..2)
     extern __shared__ __align__(16) float sm[];
     const StreamTile tl = a.tiles[blockIdx.x];
-    const int nx = a.nx, ny = a.ny, nz = a.nz, QX = nx >> 2;
+    const int nx = a.nx, ny = a.ny, nz = a.nz, QX = nx >> 2, L = a.L;
     const int TP = a.ty + 1;                         // staged rows per array
+    const int XW = stream_xpsi_stride(CPML ? L : 0); // staged x-slab auxiliaries per row (2L, padded)
     const long long nxy = (long long)nx * ny;
     const int r = (int)threadIdx.x / QX, q = (int)threadIdx.x - r * QX;
     const int R = tl.rows;
@@ -209,22 +222,26 @@ __global__ void __launch_bounds__(kStreamMaxThreads, 1) k_yee_stream(StreamArgs 
     const int i0 = 4 * q;
     const long long ij0 = (long long)i0 + (long long)nx * j;
     float *stage = sm;                               // [S][NA][TP][nx]
-    float *hlow = sm + (size_t)S * NA * TP * nx;     // [S][2][nx]: Hx, Hz of row j0-1
+    float *xps = stage + (size_t)S * NA * TP * nx;   // [S][4][TP][XW]: x-slab auxiliaries E0 E1 H0 H1
+    float *hlow = xps + (size_t)S * 4 * TP * XW;     // [S][2][nx]: Hx, Hz of row j0-1
     float *es = hlow + (size_t)S * 2 * nx;           // [2][3][TP][nx]: new E of the last two planes
     auto stg = [&](int s, int arr, int row) -> float * { return stage + ((size_t)(s * NA + arr) * TP + row) * nx; };
+    auto xrow = [&](int s, int arr, int row) -> float * { return xps + ((size_t)(s * 4 + arr) * TP + row) * XW; };
     auto esp = [&](int b, int c, int row) -> float * { return es + ((size_t)(b * 3 + c) * TP + row) * nx; };
     const int n = tl.k1 - tl.k0;                     // owned planes; iterations 0..n
 
     // Copies of iteration `it` (plane k0 + it) into stage (it + S) % S, one
     // group per call.  Every thread copies only its own slots (row r, quad q;
-    // row 0 also the j0-1 slots), and other threads read those slots only in
-    // the E update of iteration `it`, after the barrier that follows the copy.
-    // `h_only`: just H (iteration -1, plane k0 - 1: the previous plane of
-    // iteration 0).
+    // row 0 also the j0-1 slots; the row's x-slab auxiliaries in pieces spread
+    // over the row's threads), and other threads read those slots only in the
+    // iteration that consumes the stage, after the barrier that follows the
+    // copy.  `h_only`: just H (iteration -1, plane k0 - 1: the previous plane
+    // of iteration 0).
     auto issue = [&](int it, bool h_only) {
         if (it <= n && act) {
             const int s = (it + S) % S;
-            const long long g = ij0 + nxy * (tl.k0 + it);
+            const int k = tl.k0 + it;
+            const long long g = ij0 + nxy * k;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 cp_async16(stg(s, c, r) + i0, a.f_in[3 + c] + g);
@@ -237,6 +254,21 @@ __global__ void __launch_bounds__(kStreamMaxThreads, 1) k_yee_stream(StreamArgs 
             if (r == 0 && !h_only) {
                 cp_async16(hlow + (size_t)(s * 2 + 0) * nx + i0, a.f_in[3] + g - nx);
                 cp_async16(hlow + (size_t)(s * 2 + 1) * nx + i0, a.f_in[5] + g - nx);
+            }
+            if (CPML && !h_only) {
+                const long long xs0 = 2LL * L * (j + (long long)ny * k);
+                if ((L & 1) == 0) {
+                    const int nch = L >> 1;              // 16-byte pieces per row of 2L
+                    for (int c = q; c < 4 * nch; c += QX) {
+                        const int arr = c / nch, ch = c - arr * nch;
+                        cp_async16(xrow(s, arr, r) + 4 * ch, a.psi_in[0][arr] + xs0 + 4 * ch);
+                    }
+                } else {
+                    for (int c = q; c < 8 * L; c += QX) {
+                        const int arr = c / (2 * L), e = c - arr * 2 * L;
+                        cp_async4(xrow(s, arr, r) + e, a.psi_in[0][arr] + xs0 + e);
+                    }
+                }
             }
         }
         cp_async_commit_group();
@@ -251,11 +283,12 @@ __global__ void __launch_bounds__(kStreamMaxThreads, 1) k_yee_stream(StreamArgs 
         const int k = tl.k0 + it;
         const int s = it % S, sp_ = (it + S - 1) % S;      // this plane's stage, the previous plane's
         const bool e_upd = act && row_upd && k <= nz - 2;   // k >= 1 always
-        // CPML state of the E update, loaded before the wait so its latency
-        // overlaps the wait for the staged planes
-        XPsi xse;
-        YZPsi yze;
-        if (CPML && e_upd) stream_psi_load<0>(xse, yze, a, q, j, k, ij0, nxy);
+        const bool h_upd = own && it >= 1;
+        // y- and z-slab auxiliaries of both updates, loaded before the wait so
+        // their latency overlaps it
+        YZPsi yze, yzh;
+        if (CPML && e_upd) stream_yzpsi_load<0>(yze, a, q, j, k, ij0, nxy);
+        if (CPML && h_upd) stream_yzpsi_load<2>(yzh, a, q, j, k - 1, ij0, nxy);
         cp_async_wait_group<1>();   // this thread's copies up to iteration it have landed
         __syncthreads();            // ... and everyone's; new E of iteration it-1 visible
 
@@ -266,7 +299,9 @@ __global__ void __launch_bounds__(kStreamMaxThreads, 1) k_yee_stream(StreamArgs 
             ey = lds4(stg(s, 4, r) + i0);
             ez = lds4(stg(s, 5, r) + i0);
         }
+        XPsi xse;
         if (e_upd) {
+            if (CPML) stream_xpsi(xse, xrow(s, 0, r), xrow(s, 1, r), nx, L, q);
             const Vf<4> hx = lds4(stg(s, 0, r) + i0), hy = lds4(stg(s, 1, r) + i0), hz = lds4(stg(s, 2, r) + i0);
             const Vf<4> hx_km = lds4(stg(sp_, 0, r) + i0), hy_km = lds4(stg(sp_, 1, r) + i0);
             const Vf<4> hx_jm = r > 0 ? lds4(stg(s, 0, r - 1) + i0) : lds4(hlow + (size_t)(s * 2 + 0) * nx + i0);
@@ -327,14 +362,14 @@ __global__ void __launch_bounds__(kStreamMaxThreads, 1) k_yee_stream(StreamArgs 
             if (CPML) stream_psi_store<0>(xse, yze, a, q, j, k, ij0, nxy);
         }
 
-        // ---- H_new(k-1) of rows j0..j0+R-1: own old H from the previous stage,
-        //      the new E of plane k-1 from the shared array of iteration it-1
-        //      (own cells and neighbours), the new E of plane k from registers
-        if (own && it >= 1) {
+        // ---- H_new(k-1) of rows j0..j0+R-1: own old H and x-slab auxiliaries
+        //      from the previous stage, the new E of plane k-1 from the shared
+        //      array of iteration it-1 (own cells and neighbours), the new E of
+        //      plane k from registers
+        if (h_upd) {
             const int km = k - 1;
             XPsi xsh;
-            YZPsi yzh;
-            if (CPML) stream_psi_load<2>(xsh, yzh, a, q, j, km, ij0, nxy);
+            if (CPML) stream_xpsi(xsh, xrow(sp_, 2, r), xrow(sp_, 3, r), nx, L, q);
             const int b = (it - 1) & 1;
             const Vf<4> exm = lds4(esp(b, 0, r) + i0), eym = lds4(esp(b, 1, r) + i0), ezm = lds4(esp(b, 2, r) + i0);
             const Vf<4> ex_jp = lds4(esp(b, 0, r + 1) + i0), ez_jp = lds4(esp(b, 2, r + 1) + i0);
@@ -379,9 +414,8 @@ __global__ void __launch_bounds__(kStreamMaxThreads, 1) k_yee_stream(StreamArgs 
             stv<4>(a.f_out[5] + g, nhz);
             if (CPML) stream_psi_store<2>(xsh, yzh, a, q, j, km, ij0, nxy);
         }
-        // Plane it+2 into the previous plane's stage: this thread has read its
-        // own slots there above (the values are consumed), and no other thread
-        // reads them any more.
+        // Plane it+2 into the previous plane's stage: this thread has consumed
+        // its own slots there above, and no other thread reads them any more.
         issue(it + 2, false);
     }
     cp_async_wait_group<0>();
@@ -390,10 +424,11 @@ __global__ void __launch_bounds__(kStreamMaxThreads, 1) k_yee_stream(StreamArgs 
 // ---------------------------------------------------------------------------
 // host side: the tile plan
 // ---------------------------------------------------------------------------
-static size_t stream_smem_floats(int nx, int ty, bool lossy)
+static size_t stream_smem_floats(int nx, int ty, bool lossy, int L)
 {
     const int NA = lossy ? 12 : 9;
-    return ((size_t)kStreamStages * NA * (ty + 1) + 2 * kStreamStages + 6 * (size_t)(ty + 1)) * nx;
+    return ((size_t)kStreamStages * NA * (ty + 1) + 2 * kStreamStages + 6 * (size_t)(ty + 1)) * nx +
+           (size_t)kStreamStages * 4 * (ty + 1) * stream_xpsi_stride(L);
 }
 
 // split items 0..n-1 of cost c[] into at most `parts` contiguous runs of at
@@ -431,20 +466,20 @@ static std::vector<int> split_runs(const std::vector<double> &c, int parts, int 
     return starts;
 }
 
-int stream_supported(int nx, int ny, int nz, bool lossy)
+int stream_supported(int nx, int ny, int nz, bool lossy, int L)
 {
-    if (nx % 4 != 0 || nx < 8 || ny < 3 || nz < 3) return 0;
+    if (nx % 4 != 0 || nx < 8 || ny < 3 || nz < 3 || L < 0) return 0;
     const int QX = nx / 4;
     if (2 * QX > kStreamMaxThreads) return 0;                      // at least one row plus its halo row
-    return stream_smem_floats(nx, 1, lossy) * sizeof(float) <= kStreamSmemBudget;
+    return stream_smem_floats(nx, 1, lossy, L) * sizeof(float) <= kStreamSmemBudget;
 }
 
 bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan *out)
 {
-    if (!stream_supported(nx, ny, nz, lossy) || nsm <= 0) return false;
+    if (!stream_supported(nx, ny, nz, lossy, L) || nsm <= 0) return false;
     const int QX = nx / 4, rows = ny - 2, planes = nz - 2;
     int ty_max = kStreamMaxThreads / QX - 1;
-    while (ty_max > 1 && stream_smem_floats(nx, ty_max, lossy) * sizeof(float) > kStreamSmemBudget) ty_max--;
+    while (ty_max > 1 && stream_smem_floats(nx, ty_max, lossy, L) * sizeof(float) > kStreamSmemBudget) ty_max--;
     ty_max = std::min(ty_max, rows);
     // bytes per cell of each row / plane (60 B, plus 32 B per CPML axis)
     std::vector<double> rc(rows), pc(planes);
@@ -486,7 +521,7 @@ bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan 
         }
     }
     out->threads = ((out->ty + 1) * QX + 31) / 32 * 32;
-    out->smem = stream_smem_floats(nx, out->ty, lossy) * sizeof(float);
+    out->smem = stream_smem_floats(nx, out->ty, lossy, L) * sizeof(float);
     return true;
 }
 

@@ -220,7 +220,8 @@ def reference_arm(args, rank: int) -> None:
 
 def config_block(args) -> dict:
     return {"workload": WORKLOAD_NAME, "grid": [W["nx"], W["ny"], W["nz"]], "dx_um": W["dx"],
-            "time_steps": args.time_steps, "cpml_cells": W["cpml"], "n_lambda": len(W["lams"]),
+            "time_steps": args.time_steps, "cpml_cells": W["cpml"] if getattr(args, "boundary", "cpml") == "cpml" else 0,
+            "n_lambda": len(W["lams"]),
             "lambda_um": [W["lams"][0], W["lams"][-1]], "fields": "f32", "monitors": "f64 compensated",
             "taper_um": [0.5, 3.0], "taper_length_um": (W["taper_z"][1] - W["taper_z"][0]) * W["dx"],
             "l2": "inputs larger than L2 (fields 307 MB, no flush needed)",
@@ -233,7 +234,7 @@ def config_block(args) -> dict:
 class Taper:
     """One simulation of the workload on one GPU."""
 
-    def __init__(self, fd, time_steps: int, variant: int = 0, precision: int | None = None):
+    def __init__(self, fd, time_steps: int, variant: int = 0, precision: int | None = None, boundary: str = "cpml"):
         self.fd, self.T = fd, time_steps
         lib = fd.lib
         nx, ny, nz, dx = W["nx"], W["ny"], W["nz"], W["dx"]
@@ -241,7 +242,10 @@ class Taper:
         self.grid = fd.Grid(nx, ny, nz, dx, fd.F32 if precision is None else precision)
         self.t = self.grid.t
         rasterise(lib, self.t)
-        fd.call("timefield3d_set_cpml", self.t, W["cpml"], 3, -1.0, 1.0, 0.0)
+        if boundary == "cpml":
+            fd.call("timefield3d_set_cpml", self.t, W["cpml"], 3, -1.0, 1.0, 0.0)
+        else:   # analysis only: the same grid with PEC walls (no CPML terms)
+            fd.call("timefield3d_set_boundary", self.t, fd.PEC)
         fd.call("timefield3d_set_yee_variant", self.t, variant)
         self.mode_in = fd.read_mode_file(os.path.join(MODES, "c1_in_te0.txt.gz"))
         self.mode_out = fd.read_mode_file(os.path.join(MODES, "c1_out_te0.txt.gz"))
@@ -326,7 +330,8 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
     ranks = importlib.import_module("3d_fdtd_b200.replicas").Ranks("nccl", timeout_s=120)
     barrier, max_over_ranks = ranks.barrier, ranks.max
 
-    sim = Taper(fd, args.time_steps, {"auto": 0, "flat": 1, "fused": 2, "flat4": 3, "wave": 4, "stream": 5}[args.yee_variant])
+    sim = Taper(fd, args.time_steps, {"auto": 0, "flat": 1, "fused": 2, "flat4": 3, "wave": 4, "stream": 5}[args.yee_variant],
+                boundary=args.boundary)
     stream = torch.cuda.ExternalStream(fd.lib.timefield3d_get_stream(sim.t))
     cells = W["nx"] * W["ny"] * W["nz"]
     # warm-up: full runs (graph capture, clocks)
@@ -363,7 +368,7 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
     trans = sim.transmission()
     # roofline of the Yee update (E + H kernels with CPML), measured inside the timed runs
     kms = ktot.value / max(kcnt.value, 1)
-    bytes_step = algorithmic_bytes_per_step(W["nx"], W["ny"], W["nz"], W["cpml"])
+    bytes_step = algorithmic_bytes_per_step(W["nx"], W["ny"], W["nz"], W["cpml"] if args.boundary == "cpml" else 0)
     achieved = bytes_step / (kms / 1e3) / 1e9
     peak, peak_kind = peaks()
     wave = args.yee_variant == "wave"
@@ -384,7 +389,7 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
     t32 = sim.amplitude_ratio()
     f64_check = None
     if not args.no_f64_check:
-        ref64 = Taper(fd, args.time_steps, 0, fd.F64)
+        ref64 = Taper(fd, args.time_steps, 0, fd.F64, boundary=args.boundary)
         ref64.run()
         t64 = ref64.amplitude_ratio()
         ref64.close()
@@ -437,6 +442,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-f64-check", action="store_true", help="skip the FP64 run that checks the FP32 transmission")
+    ap.add_argument("--boundary", choices=["cpml", "pec"], default="cpml",
+                    help="pec: analysis of the update without CPML terms (not the bench workload)")
     ap.add_argument("--yee-variant", choices=["auto", "flat", "flat4", "fused", "wave", "stream"], default="auto")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))

@@ -146,6 +146,7 @@ SIGNATURES = {
     "timefield3d_step_count": (ll, [T]),
     "timefield3d_set_source_schedule": (i, [T, i, i, i, M, i, i, i, dp, dp]),
     "timefield3d_clear_source_schedule": (i, [T]),
+    "timefield3d_set_exact_adjoint_schedule": (i, [T, i, i, i, M, i, i, d, d, d, d]),
     "adjoint3d_taper_bind_store": (i, [P, T, i, i, i]),
     "adjoint3d_taper_unbind_store": (i, [P, T]),
     "timefield3d_run": (i, [T, d, i]),
@@ -180,6 +181,7 @@ SIGNATURES = {
     "fdtd_spline_store_bind": (i, [C.c_void_p, T, i, i, i]),
     "fdtd_spline_store_unbind": (i, [C.c_void_p, T]),
     "fdtd_spline_store_gradient": (i, [C.c_void_p, d, dp, dp]),
+    "fdtd_spline_store_gradient_exact": (i, [C.c_void_p, d, dp, dp]),
     "fdtd_spline_store_free": (None, [C.c_void_p]),
     "timefield3d_get_stream": (C.c_void_p, [T]),
     "timefield3d_upload_materials": (i, [T]),

@@ -12,9 +12,8 @@ namespace fdtd {
 __global__ void k_mode_source(SourceJob sj, double amplitude, double cph, double sph, const long long *step,
                               int step_offset)
 {
-    double A = amplitude, c = cph, s = sph;
-    if (sj.sched) schedule_values(sj, *step + step_offset, A, c, s);
-    mode_source_cells(sj, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x, A, c, s);
+    const SrcStep v = sj.sched ? schedule_step(sj, *step + step_offset) : fixed_step(amplitude, cph, sph);
+    mode_source_cells(sj, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x, v);
 }
 
 __global__ void k_set_value(float *p, long long idx, float v) { p[idx] = v; }
@@ -87,10 +86,9 @@ __global__ void __launch_bounds__(256) k_step_tail(TailArgs a)
         const OverlapJob jb = a.jobs[jid];
         overlap_block<T>((const T *const *)a.f, a.nx, a.ny, jb, part, a.nparts, a.partials + b);
     } else {
-        double A, c, s;
-        schedule_values(a.src, *a.step + 1, A, c, s);
+        const SrcStep v = schedule_step(a.src, *a.step + 1);
         mode_source_cells(a.src, (b - nov) * (long long)blockDim.x + threadIdx.x,
-                          (long long)a.src_blocks * blockDim.x, A, c, s);
+                          (long long)a.src_blocks * blockDim.x, v);
     }
     __shared__ bool last;
     __threadfence();
@@ -224,6 +222,41 @@ __global__ void k_ep_gradient(const T *fwd, const T *adj, int ncell, int duratio
     }
     grad[c] = sum;
 }
+
+// Exact discrete-adjoint ep-gradient: dF/deps of each stored cell (summed over
+// its 3 E components) for a forward store fwd[n] = E after forward step n and
+// an adjoint store adj[n] = the exact adjoint's E at forward index n (see
+// timefield3d_set_exact_adjoint_schedule):
+//   g = -sum_{n=0}^{T-1} adj[n] (fwd[n] - fwd[n-1]),  fwd[-1] = 0.
+// A change deps of a cell changes its E update in forward step n by
+// -(deps/eps)(E^{n+1} - E^n); the objective's sensitivity to a change of E made
+// during step n is eps times the adjoint E of index n (the state before step
+// n), so eps cancels.
+template <typename T>
+__global__ void k_ep_gradient_exact(const T *fwd, const T *adj, int ncell, int duration, double *grad)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    double sum = 0.0;
+    for (int t = 0; t < duration; t++) {
+        const long long o = ((long long)t * ncell + c) * 3, om = o - 3LL * ncell;
+#pragma unroll
+        for (int m = 0; m < 3; m++) {
+            const double d = t > 0 ? dsub((double)fwd[o + m], (double)fwd[om + m]) : (double)fwd[o + m];
+            sum = dadd(sum, dmul((double)adj[o + m], d));
+        }
+    }
+    grad[c] = -sum;
+}
+
+template <typename T> void launch_ep_gradient_exact(const T *fwd, const T *adj, int ncell, int duration, double *grad,
+                                                    cudaStream_t st)
+{
+    note_launch();
+    k_ep_gradient_exact<T><<<(ncell + 127) / 128, 128, 0, st>>>(fwd, adj, ncell, duration, grad);
+}
+template void launch_ep_gradient_exact<float>(const float *, const float *, int, int, double *, cudaStream_t);
+template void launch_ep_gradient_exact<double>(const double *, const double *, int, int, double *, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // materials: finite check (one flag), and FP32 update coefficients

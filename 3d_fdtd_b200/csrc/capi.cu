@@ -1133,6 +1133,53 @@ int timefield3d_set_source_schedule(timefield3d psi, int center_x, int center_y,
     return FDTD_OK;
 }
 
+int timefield3d_set_exact_adjoint_schedule(timefield3d psi, int center_x, int center_y, int center_z,
+                                           mode monitor_mode, int reverse, int nsteps, double omega, double delta_t,
+                                           double weight_re, double weight_im)
+{
+    LOCK;
+    Grid *g = dev_grid(psi);
+    if (!g) return fdtd_last_error();
+    if (!check_mode_plane(g, center_z)) return FDTD_ERR_ARG;
+    if (nsteps <= 0 || !(delta_t > 0) || !std::isfinite(omega) || !std::isfinite(weight_re) ||
+        !std::isfinite(weight_im)) {
+        set_error(FDTD_ERR_ARG, "exact adjoint schedule needs nsteps > 0, delta_t > 0 and finite omega and weight");
+        return FDTD_ERR_ARG;
+    }
+    if (!cuda_ok(cudaStreamSynchronize(g->st), "sync")) return fdtd_last_error();
+    if (g->sched.active) {
+        cudaFree(g->sched.d_sched);
+        priv_mode_free(g->sched.mode_key);
+        g->sched = Schedule{};
+    }
+    // nsteps + 1 entries: entry u drives the E-update current of adjoint step u
+    // (the monitor's weights of forward step nsteps - u, none for u = 0) and the
+    // H-update current of step u - 1 (forward step nsteps - u)
+    const int n = nsteps + 1;
+    std::vector<double> tab(3 * (size_t)n);
+    for (int u = 0; u < n; u++) {
+        const double ph = omega * delta_t * (double)(nsteps - u);
+        tab[3 * u] = u >= 1 ? 1.0 : 0.0;
+        tab[3 * u + 1] = cos(ph);
+        tab[3 * u + 2] = sin(ph);
+    }
+    Schedule sc{};
+    sc.cx = center_x; sc.cy = center_y; sc.cz = center_z; sc.reverse = reverse; sc.adjoint = 2; sc.n = n;
+    sc.kappa = 0.5 * g->dx * g->dx / delta_t;
+    sc.wre = weight_re;
+    sc.wim = weight_im;
+    sc.mode_key = priv_mode_new(monitor_mode);
+    if (!sc.mode_key) return fdtd_last_error();
+    if (!cuda_ok(cudaMalloc(&sc.d_sched, tab.size() * sizeof(double)), "cudaMalloc(schedule)")) return fdtd_last_error();
+    if (!cuda_ok(cudaMemcpy(sc.d_sched, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice), "schedule H2D"))
+        return fdtd_last_error();
+    sc.active = true;
+    g->sched = sc;
+    if (!grid_plane(g, center_z, true)) return fdtd_last_error();
+    g->version++;
+    return FDTD_OK;
+}
+
 int timefield3d_clear_source_schedule(timefield3d psi)
 {
     LOCK;

@@ -698,8 +698,9 @@ static bool stream_prepare(Grid *g)
         set_error(FDTD_ERR_UNSUPPORTED, "streaming Yee kernel: no tile plan for grid %dx%dx%d", g->nx, g->ny, g->nz);
         return false;
     }
-    if (!stream_configure(p.smem)) {
-        set_error(FDTD_ERR_CUDA, "streaming Yee kernel: %zu bytes of shared memory per block refused", p.smem);
+    if (!stream_configure(p.smem, p.threads)) {
+        set_error(FDTD_ERR_CUDA, "streaming Yee kernel: blocks of %d threads with %zu bytes of shared memory cannot launch",
+                  p.threads, p.smem);
         return false;
     }
     CK(cudaStreamSynchronize(g->st));
@@ -1080,6 +1081,7 @@ static bool schedule_job(Grid *g, SourceJob *sj)
     sj->ratio = g->dx / it->second.disc;
     sj->sched = g->sched.d_sched; sj->nsched = g->sched.n;
     sj->reverse = g->sched.reverse; sj->adjoint = g->sched.adjoint;
+    sj->kappa = g->sched.kappa; sj->wre = g->sched.wre; sj->wim = g->sched.wim;
     return true;
 }
 

@@ -71,6 +71,7 @@ struct ProbeRec {
 struct Schedule {
     bool active = false;
     int cx, cy, cz, reverse, adjoint, n;
+    double kappa = 0, wre = 1, wim = 0;   // exact adjoint (adjoint 2)
     const void *mode_key = nullptr;
     double *d_sched = nullptr;   // 3*n: amplitude, cos, sin
 };

@@ -80,7 +80,8 @@ struct SourceJob {
     double ratio;
     const double *sched;
     int nsched;
-    int reverse, adjoint;
+    int reverse, adjoint;       // adjoint 2: exact discrete adjoint of an overlap monitor (see plane_ops.cuh)
+    double kappa, wre, wim;     // adjoint 2: disc^2 / (2 delta_t) and the complex weight of the objective
     ModeWindow win;             // set by launch_mode_source_job / the tail launcher
 };
 
@@ -215,8 +216,9 @@ __host__ __device__ inline int stream_xpsi_stride(int L) { return (2 * L + 3) & 
 int stream_supported(int nx, int ny, int nz, bool lossy, int L);
 // tiles for a grid on a device with nsm SMs; false when the grid cannot use the kernel
 bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan *out);
-// allow `smem` bytes of dynamic shared memory for every instantiation (host, not stream-ordered)
-bool stream_configure(size_t smem);
+// allow `smem` bytes of dynamic shared memory for every instantiation and check
+// that blocks of `threads` threads can launch (host, not stream-ordered)
+bool stream_configure(size_t smem, int threads);
 void launch_yee_stream(const StreamArgs &a, const StreamPlan &p, cudaStream_t st);
 
 // yee_wave.cu: S steps of the flat4 update in one persistent, cooperative
@@ -304,6 +306,8 @@ void launch_taper_store(const T *const *f_dev, const long long *cells, int ncell
                         const long long *step, int t0, int dir, int duration, cudaStream_t st);
 template <typename T>
 void launch_ep_gradient(const T *fwd, const T *adj, int ncell, int duration, double *grad, cudaStream_t st);
+template <typename T>
+void launch_ep_gradient_exact(const T *fwd, const T *adj, int ncell, int duration, double *grad, cudaStream_t st);
 void launch_check_finite(const float *a, long long n, int *bad, cudaStream_t st);
 
 // umma_gemm.cu: BF16 GEMM on tcgen05 (pre = alpha A B^T + beta C32 + bias;

@@ -31,10 +31,54 @@ __device__ __forceinline__ void schedule_values(const SourceJob &sj, long long n
     }
 }
 
+// amplitude and phase of a source plane: entry n of the schedule, and for the
+// exact adjoint (adjoint 2) also entry n+1, which drives the H components
+struct SrcStep {
+    double A, c, s;       // J (E components); all six components otherwise
+    double A1, c1, s1;    // M (H components) of the exact adjoint
+};
+
+__device__ __forceinline__ SrcStep schedule_step(const SourceJob &sj, long long n)
+{
+    SrcStep v;
+    schedule_values(sj, n, v.A, v.c, v.s);
+    if (sj.adjoint == 2) schedule_values(sj, n + 1, v.A1, v.c1, v.s1);
+    else { v.A1 = 0.0; v.c1 = 0.0; v.s1 = 0.0; }
+    return v;
+}
+
+__device__ __forceinline__ SrcStep fixed_step(double A, double c, double s)
+{
+    SrcStep v;
+    v.A = A; v.c = c; v.s = s; v.A1 = 0.0; v.c1 = 0.0; v.s1 = 0.0;
+    return v;
+}
+
+// Re(w m e^{i phi}) for a mode sample m, with (c, s) = (cos phi, sin phi)
+__device__ __forceinline__ double weighted_proj(const SourceJob &sj, double2 m, double c, double s)
+{
+    const double zr = dsub(dmul(sj.wre, m.x), dmul(sj.wim, m.y));
+    const double zi = dadd(dmul(sj.wre, m.y), dmul(sj.wim, m.x));
+    return dsub(dmul(zr, c), dmul(zi, s));
+}
+
 // the six source values of cell (i, j); false when the cell has no mode
 // sample (the plane keeps its value there)
-__device__ __forceinline__ bool mode_source_cell(const SourceJob &sj, int i, int j, double A, double c, double s,
-                                                 float v[6])
+//   adjoint 0: timefield3d_mode_source (timefield3d.c:2977-3026)
+//   adjoint 1: timefield3d_mode_source_adjoint (timefield3d.c:3028-3068)
+//   adjoint 2: the exact discrete adjoint of an overlap monitor
+//     O = sum_n e^{i omega n dt} o_n, o_n = -disc^2/2 sum (Hx mEy - Hy mEx + Ey mHx - Ex mHy)
+//     (mode H -> -conj(H) when reverse) for the objective Re(w O): with
+//     kappa = disc^2 / (2 dt), the E-update current
+//       Jx = -kappa Re(w mHy e^{i phi_n}), Jy = kappa Re(w mHx e^{i phi_n})
+//     adds exactly the monitor's E weights (divided by eps) to E, and the
+//     H-update current of entry n+1
+//       Mx = -kappa Re(w mEy e^{i phi_n+1}), My = kappa Re(w mEx e^{i phi_n+1})
+//     adds minus its H weights at the end of the step, i.e. before the next
+//     step's E update (the transposed leapfrog step is the same step with H
+//     negated, so the adjoint is this forward run; see
+//     timefield3d_set_exact_adjoint_schedule).
+__device__ __forceinline__ bool mode_source_cell(const SourceJob &sj, int i, int j, const SrcStep &st, float v[6])
 {
     const long long t = i + (long long)sj.nx * j;
     const int M_sign = -1 + 2 * sj.reverse;
@@ -43,7 +87,8 @@ __device__ __forceinline__ bool mode_source_cell(const SourceJob &sj, int i, int
     int mx = (int)xd + sj.mi / 2, my = (int)yd + sj.mj / 2;
     if (mx < 0 || mx >= sj.mi || my < 0 || my >= sj.mj) return false;
     const double2 *e = sj.mode + 6LL * (mx + (long long)sj.mi * my);
-    if (!sj.adjoint) {
+    const double A = st.A, c = st.c, s = st.s;
+    if (sj.adjoint == 0) {
 #pragma unroll
         for (int m = 0; m < 6; m++) {
             double proj = dadd(dmul(e[m].x, c), dmul(e[m].y, s));
@@ -52,20 +97,33 @@ __device__ __forceinline__ bool mode_source_cell(const SourceJob &sj, int i, int
             else w = dmul(dmul(dmul((double)(-M_sign), A), (double)sj.mu[m - 3][t]), proj);
             v[m] = __double2float_rn(w);
         }
-    } else {
+    } else if (sj.adjoint == 1) {
         v[0] = __double2float_rn(dmul(1.0, dadd(dmul(e[4].x, c), dmul(e[4].y, s))));
         v[1] = __double2float_rn(dmul(-1.0, dadd(dmul(e[3].x, c), dmul(e[3].y, s))));
         v[2] = 0.0f;
         v[3] = __double2float_rn(dmul((double)(-1 * M_sign), dadd(dmul(e[1].x, c), dmul(e[1].y, s))));
         v[4] = __double2float_rn(dmul((double)(1 * M_sign), dadd(dmul(e[0].x, c), dmul(e[0].y, s))));
         v[5] = 0.0f;
+    } else {
+        double2 mHx = e[3], mHy = e[4];
+        if (sj.reverse) {
+            mHx.x = -mHx.x;
+            mHy.x = -mHy.x;
+        }
+        const double k0 = dmul(sj.kappa, A), k1 = dmul(sj.kappa, st.A1);
+        v[0] = __double2float_rn(-dmul(k0, weighted_proj(sj, mHy, c, s)));
+        v[1] = __double2float_rn(dmul(k0, weighted_proj(sj, mHx, c, s)));
+        v[2] = 0.0f;
+        v[3] = __double2float_rn(-dmul(k1, weighted_proj(sj, e[1], st.c1, st.s1)));
+        v[4] = __double2float_rn(dmul(k1, weighted_proj(sj, e[0], st.c1, st.s1)));
+        v[5] = 0.0f;
     }
     return true;
 }
 
-// window cells u = first, first + stride, ... of the source plane
-__device__ __forceinline__ void mode_source_cells(const SourceJob &sj, long long first, long long stride, double A,
-                                                  double c, double s)
+// the source plane over the mode window, cells first, first + stride, ...
+__device__ __forceinline__ void mode_source_cells(const SourceJob &sj, long long first, long long stride,
+                                                  const SrcStep &st)
 {
     const long long nxy = (long long)sj.nx * sj.ny;
     const long long cells = (long long)sj.win.wni * sj.win.wnj;
@@ -73,7 +131,7 @@ __device__ __forceinline__ void mode_source_cells(const SourceJob &sj, long long
         const int i = sj.win.wi + (int)(u % sj.win.wni), j = sj.win.wj + (int)(u / sj.win.wni);
         const long long t = i + (long long)sj.nx * j;
         float v[6];
-        if (!mode_source_cell(sj, i, j, A, c, s, v)) continue;
+        if (!mode_source_cell(sj, i, j, st, v)) continue;
 #pragma unroll
         for (int m = 0; m < 6; m++) sj.plane[m * nxy + t] = v[m];
     }

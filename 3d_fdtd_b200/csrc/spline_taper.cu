@@ -372,7 +372,19 @@ int fdtd_spline_store_unbind(fdtd_spline_store store, timefield3d psi)
     return FDTD_OK;
 }
 
+static int spline_gradient(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient, bool exact);
+
 int fdtd_spline_store_gradient(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient)
+{
+    return spline_gradient(store, ep_diff, grad, cell_gradient, false);
+}
+
+int fdtd_spline_store_gradient_exact(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient)
+{
+    return spline_gradient(store, ep_diff, grad, cell_gradient, true);
+}
+
+static int spline_gradient(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient, bool exact)
 {
     std::lock_guard<std::mutex> lock(api_mutex());
     auto *s = (SplineStore *)store;
@@ -382,7 +394,13 @@ int fdtd_spline_store_gradient(fdtd_spline_store store, double ep_diff, double *
         return FDTD_ERR_ARG;
     }
     if (!cuda_ok(cudaDeviceSynchronize(), "sync")) return fdtd_last_error();
-    if (td->prec == FDTD_F64)
+    if (exact && td->prec == FDTD_F64)
+        launch_ep_gradient_exact<double>((const double *)td->d_fwd, (const double *)td->d_adj, td->ncell,
+                                         td->duration, td->d_grad, 0);
+    else if (exact)
+        launch_ep_gradient_exact<float>((const float *)td->d_fwd, (const float *)td->d_adj, td->ncell, td->duration,
+                                        td->d_grad, 0);
+    else if (td->prec == FDTD_F64)
         launch_ep_gradient<double>((const double *)td->d_fwd, (const double *)td->d_adj, td->ncell, td->duration,
                                    td->d_grad, 0);
     else

@@ -30,13 +30,13 @@
 // recomputed row or plane on the shell passes its E through unchanged.
 //
 // Pipeline.  Each thread owns 4 consecutive x cells of one row and moves them
-// with 16-byte cp.async copies into a ring of 3 shared-memory stages: while
-// plane k computes, plane k+1 is in flight and plane k+2 is issued at the end
-// of the iteration, into the stage of plane k-1 once the thread has used its
-// own old H there (the H update's base value).  One block barrier per plane:
+// with 16-byte cp.async copies into a ring of 3 shared-memory stages: right
+// after the plane's barrier each thread reads its own slots of plane k-1's
+// stage (old H, the H update's x-slab auxiliaries) into registers and issues
+// plane k+2 into that stage, so planes k+1 and k+2 are in flight while plane k
+// computes.  Every thread copies into its own slots only.  One block barrier per plane:
 // the new E of a plane goes to a double-buffered shared array read by the next
-// iteration's H update (own cells, neighbour rows and columns).  Nothing is
-// carried in registers from one plane to the next.  Threads of row 0 also
+// iteration's H update (own cells, neighbour rows and columns).  Threads of row 0 also
 // stage Hx, Hz of row j0-1 (the E update's j-1 neighbours); x neighbours come
 // from the same shared rows.  CPML auxiliaries and source planes are read
 // straight from global memory where a cell needs them (slab cells, source
@@ -51,7 +51,9 @@
 namespace fdtd {
 
 constexpr int kStreamStages = 3;
-constexpr int kStreamMaxThreads = 416;   // up to 152 registers a thread at one block per SM
+// 12 warps: up to 168 registers a thread at one block per SM (warps take
+// registers in groups of 4, so 13 warps would leave only 128)
+constexpr int kStreamMaxThreads = 384;
 
 __device__ __forceinline__ void cp_async16(float *smem, const float *gmem)
 {
@@ -201,7 +203,7 @@ __device__ __forceinline__ void cp_async4(float *smem, const float *gmem)
 }
 
 template <bool CPML, bool LOSSY>
-__global__ void __maxnreg__(152) k_yee_stream(StreamArgs a)
+__global__ void __launch_bounds__(kStreamMaxThreads, 1) k_yee_stream(StreamArgs a)
 {
     // programmatic dependent launch, as the flat kernels (see k_flat4_merged)
     asm volatile("griddepcontrol.wait;" ::: "memory");
@@ -255,19 +257,15 @@ __global__ void __maxnreg__(152) k_yee_stream(StreamArgs a)
                 cp_async16(hlow + (size_t)(s * 2 + 0) * nx + i0, a.f_in[3] + g - nx);
                 cp_async16(hlow + (size_t)(s * 2 + 1) * nx + i0, a.f_in[5] + g - nx);
             }
-            if (CPML && !h_only) {
+            if (CPML && !h_only && (i0 < L || i0 + 3 >= nx - L)) {
+                // this quad's own x-slab auxiliaries (4 arrays, one slot per element)
                 const long long xs0 = 2LL * L * (j + (long long)ny * k);
-                if ((L & 1) == 0) {
-                    const int nch = L >> 1;              // 16-byte pieces per row of 2L
-                    for (int c = q; c < 4 * nch; c += QX) {
-                        const int arr = c / nch, ch = c - arr * nch;
-                        cp_async16(xrow(s, arr, r) + 4 * ch, a.psi_in[0][arr] + xs0 + 4 * ch);
-                    }
-                } else {
-                    for (int c = q; c < 8 * L; c += QX) {
-                        const int arr = c / (2 * L), e = c - arr * 2 * L;
-                        cp_async4(xrow(s, arr, r) + e, a.psi_in[0][arr] + xs0 + e);
-                    }
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int si = slab_local(i0 + e, nx, L);
+                    if (si < 0) continue;
+#pragma unroll
+                    for (int arr = 0; arr < 4; arr++) cp_async4(xrow(s, arr, r) + si, a.psi_in[0][arr] + xs0 + si);
                 }
             }
         }
@@ -291,6 +289,19 @@ __global__ void __maxnreg__(152) k_yee_stream(StreamArgs a)
         if (CPML && h_upd) stream_yzpsi_load<2>(yzh, a, q, j, k - 1, ij0, nxy);
         cp_async_wait_group<1>();   // this thread's copies up to iteration it have landed
         __syncthreads();            // ... and everyone's; new E of iteration it-1 visible
+        // own slots of the previous plane's stage: old H (the E update's z
+        // neighbours, the H update's base value) and the H update's x-slab
+        // auxiliaries; then that stage takes plane it+2 (other threads read
+        // these slots only in iteration it-1, which every thread has left)
+        Vf<4> hxm = fillv<4>(0.f), hym = hxm, hzm = hxm;
+        if (act) {
+            hxm = lds4(stg(sp_, 0, r) + i0);
+            hym = lds4(stg(sp_, 1, r) + i0);
+            hzm = lds4(stg(sp_, 2, r) + i0);
+        }
+        XPsi xsh;
+        if (CPML && h_upd) stream_xpsi(xsh, xrow(sp_, 2, r), xrow(sp_, 3, r), nx, L, q);
+        issue(it + 2, false);
 
         // ---- E_new(k) of rows j0..j0+R
         Vf<4> ex = fillv<4>(0.f), ey = ex, ez = ex;
@@ -303,7 +314,7 @@ __global__ void __maxnreg__(152) k_yee_stream(StreamArgs a)
         if (e_upd) {
             if (CPML) stream_xpsi(xse, xrow(s, 0, r), xrow(s, 1, r), nx, L, q);
             const Vf<4> hx = lds4(stg(s, 0, r) + i0), hy = lds4(stg(s, 1, r) + i0), hz = lds4(stg(s, 2, r) + i0);
-            const Vf<4> hx_km = lds4(stg(sp_, 0, r) + i0), hy_km = lds4(stg(sp_, 1, r) + i0);
+            const Vf<4> hx_km = hxm, hy_km = hym;
             const Vf<4> hx_jm = r > 0 ? lds4(stg(s, 0, r - 1) + i0) : lds4(hlow + (size_t)(s * 2 + 0) * nx + i0);
             const Vf<4> hz_jm = r > 0 ? lds4(stg(s, 2, r - 1) + i0) : lds4(hlow + (size_t)(s * 2 + 1) * nx + i0);
             const float hy_im0 = q > 0 ? stg(s, 1, r)[i0 - 1] : 0.f;
@@ -368,14 +379,12 @@ __global__ void __maxnreg__(152) k_yee_stream(StreamArgs a)
         //      plane k from registers
         if (h_upd) {
             const int km = k - 1;
-            XPsi xsh;
-            if (CPML) stream_xpsi(xsh, xrow(sp_, 2, r), xrow(sp_, 3, r), nx, L, q);
             const int b = (it - 1) & 1;
             const Vf<4> exm = lds4(esp(b, 0, r) + i0), eym = lds4(esp(b, 1, r) + i0), ezm = lds4(esp(b, 2, r) + i0);
             const Vf<4> ex_jp = lds4(esp(b, 0, r + 1) + i0), ez_jp = lds4(esp(b, 2, r + 1) + i0);
             const float ey_ipw = q < QX - 1 ? esp(b, 1, r)[i0 + 4] : 0.f;
             const float ez_ipw = q < QX - 1 ? esp(b, 2, r)[i0 + 4] : 0.f;
-            Vf<4> nhx = lds4(stg(sp_, 0, r) + i0), nhy = lds4(stg(sp_, 1, r) + i0), nhz = lds4(stg(sp_, 2, r) + i0);
+            Vf<4> nhx = hxm, nhy = hym, nhz = hzm;
             const float *sp = a.src.n ? src_plane(a.src, km) : nullptr;
 #pragma unroll
             for (int e = 0; e < 4; e++) {
@@ -414,9 +423,6 @@ __global__ void __maxnreg__(152) k_yee_stream(StreamArgs a)
             stv<4>(a.f_out[5] + g, nhz);
             if (CPML) stream_psi_store<2>(xsh, yzh, a, q, j, km, ij0, nxy);
         }
-        // Plane it+2 into the previous plane's stage: this thread has consumed
-        // its own slots there above, and no other thread reads them any more.
-        issue(it + 2, false);
     }
     cp_async_wait_group<0>();
 }
@@ -525,13 +531,16 @@ bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan 
     return true;
 }
 
-bool stream_configure(size_t smem)
+bool stream_configure(size_t smem, int threads)
 {
     if (smem > kStreamSmemBudget) return false;
     const void *fns[4] = {(const void *)k_yee_stream<false, false>, (const void *)k_yee_stream<false, true>,
                           (const void *)k_yee_stream<true, false>, (const void *)k_yee_stream<true, true>};
-    for (const void *f : fns)
+    for (const void *f : fns) {
         if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
+        cudaFuncAttributes at{};
+        if (cudaFuncGetAttributes(&at, f) != cudaSuccess || at.maxThreadsPerBlock < threads) return false;
+    }
     return true;
 }
 

@@ -235,14 +235,13 @@ __global__ void __launch_bounds__(kBlock4, 3) k_wave(FlatArgs a, Plan4 p, WaveAr
 __global__ void k_wave_ring(SourceJob sj, float *ring, long long stride, const long long *step)
 {
     const int ls = blockIdx.y;
-    double A, c, s;
-    schedule_values(sj, *step + ls, A, c, s);
+    const SrcStep sv = schedule_step(sj, *step + ls);
     const long long nxy = (long long)sj.nx * sj.ny;
     float *dst = ring + ls * stride;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nxy; t += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(t % sj.nx), j = (int)(t / sj.nx);
         float v[6];
-        if (!mode_source_cell(sj, i, j, A, c, s, v)) {
+        if (!mode_source_cell(sj, i, j, sv, v)) {
 #pragma unroll
             for (int m = 0; m < 6; m++) v[m] = sj.plane[m * nxy + t];
         }
@@ -307,10 +306,9 @@ __global__ void __launch_bounds__(256) k_wave_finalize(WaveFinal f)
             }
         }
     } else if (f.src.plane) {
-        double A, c, s;
-        schedule_values(f.src, n0 + f.steps, A, c, s);
+        const SrcStep sv = schedule_step(f.src, n0 + f.steps);
         mode_source_cells(f.src, (blockIdx.x - f.njobs) * (long long)blockDim.x + tid,
-                          (long long)(gridDim.x - f.njobs) * blockDim.x, A, c, s);
+                          (long long)(gridDim.x - f.njobs) * blockDim.x, sv);
     }
     __shared__ bool last;
     __threadfence();

@@ -316,6 +316,23 @@ long long timefield3d_step_count(timefield3d psi);
  * Applied by timefield3d_run. */
 int timefield3d_set_source_schedule(timefield3d psi, int center_x, int center_y, int center_z, mode source_mode, int reverse, int adjoint, int nsteps, const double *amplitude, const double *phase);
 int timefield3d_clear_source_schedule(timefield3d psi);
+/* Exact discrete adjoint of an overlap monitor.  No reference counterpart:
+ * it replaces the reference driver's CW adjoint (3d_fdtd.c:143-165 with
+ * timefield3d_mode_source_adjoint) when the gradient must equal the derivative
+ * of the simulated objective.  For a forward run of nsteps steps from zero
+ * fields whose monitor (this mode at center_x/y/z, `reverse` as for
+ * timefield3d_add_overlap_monitor) accumulates O(omega), and the objective
+ * F = Re(w O) with w = weight_re + i weight_im (F = |O| at the forward design:
+ * w = conj(O)/|O|), this schedules the adjoint sources so that
+ * timefield3d_run(psi, delta_t, nsteps + 1) from zero fields runs the exact
+ * adjoint of the leapfrog scheme (the transposed step is the same step with H
+ * negated); a spline store bound with which = 1, t0 = nsteps, dir = -1 then
+ * holds the adjoint fields for fdtd_spline_store_gradient_exact.  The CPML
+ * terms run forward in the adjoint too, so the result is exact up to the
+ * absorber's reflection. */
+int timefield3d_set_exact_adjoint_schedule(timefield3d psi, int center_x, int center_y, int center_z,
+                                           mode monitor_mode, int reverse, int nsteps, double omega, double delta_t,
+                                           double weight_re, double weight_im);
 /* Bind a taper's edge store to timefield3d_run: after step n the edge fields
  * are stored at time index t0 + dir*n (which = 0 forward, 1 adjoint). */
 int adjoint3d_taper_bind_store(adjoint3d_taper taper, timefield3d psi, int which, int t0, int dir);
@@ -377,6 +394,13 @@ int fdtd_spline_store_unbind(fdtd_spline_store store, timefield3d psi);
  * g = sum_t sum_m E_fwd E_adj at the edge cells; cell_gradient (optional,
  * 2*(top-bottom)*(end_z-start_z) values) receives g */
 int fdtd_spline_store_gradient(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient);
+/* dF/d(control width) for a forward store (which 0, t0 0, dir 1) and an adjoint
+ * store from timefield3d_set_exact_adjoint_schedule: per edge cell
+ * g = -sum_n sum_m adj[n] (fwd[n] - fwd[n-1]) (dF/deps of the cell), then the
+ * spline-weighted reduction of fdtd_spline_store_gradient.  No fitted or
+ * omitted constant: the derivative of the simulated objective.  No reference
+ * counterpart (generalises adjoint3d.c:339-418). */
+int fdtd_spline_store_gradient_exact(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient);
 void fdtd_spline_store_free(fdtd_spline_store store);
 
 /* BF16 GEMM on the tcgen05 tensor cores (no reference counterpart; the

@@ -283,6 +283,34 @@ def test_wg_adjoint_gradient_golden(fd, orc, gpu):
     fd.lib.adjoint3d_taper_free(taper)
 
 
+def test_wg_adjoint_gradient_f32_fields(fd, orc, gpu):
+    """The reference's gradient path (adjoint3d.c:339-418) on FP32 fields: the
+    ep gradient and the vertex gradients within 1e-2 of the FP64 reference."""
+    r = gpu_wg_forward(fd, fd.F32)
+    gold, p, grid, taper, outm = r["gold"], r["p"], r["grid"], r["taper"], r["outm"]
+    lib = fd.lib
+    rot = orc.cexp(float(gold["tphase"]) + fd.REF_PI / 2)
+    fr, fi = outm.fields.real.copy(), outm.fields.imag.copy()
+    outm.fields.real[...] = rot.real * fr - rot.imag * fi
+    outm.fields.imag[...] = rot.real * fi + rot.imag * fr
+    lib.timefield3d_zero_fields(grid.t)
+    T = p["steps"]
+    for n in range(T - 1, -1, -1):
+        phase = (n + 1) * r["dt"] * r["omega"]
+        lib.timefield3d_mode_source_adjoint(grid.t, r["cx"], r["cy"], p["out_z"], outm.struct, phase, 0)
+        lib.timefield3d_apply_timestep_omp_full(grid.t, r["dt"])
+        lib.adjoint3d_taper_store_adjoint_fields(taper, grid.t, n)
+    fd.check("adjoint loop")
+    fd.call("adjoint3d_taper_calculate_ep_gradient", taper)
+    n = gold["ep_grad"].size
+    assert rel(np.ctypeslib.as_array(taper.ep_gradient, shape=(n,)), gold["ep_grad"]) < 1e-2
+    fd.call("adjoint3d_taper_calculate_gradients_from_ep_gradient", taper, p["ep_core"] - p["ep_clad"])
+    S = p["seg_num"] + 1
+    assert rel(np.ctypeslib.as_array(taper.left_grad, shape=(S,)), gold["left_grad"]) < 1e-2
+    assert rel(np.ctypeslib.as_array(taper.right_grad, shape=(S,)), gold["right_grad"]) < 1e-2
+    fd.lib.adjoint3d_taper_free(taper)
+
+
 def test_kernel_timing_run_equals_untimed(fd, gpu):
     """Timed graphs (event pairs around each Yee update), on every replay or on
     one replay in 3, compute the same fields as the untimed run."""

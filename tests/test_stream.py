@@ -54,7 +54,7 @@ def test_stream_plan_covers_interior_once(fd, nx, ny, nz, L, lossy, nsm):
     assert p is not None
     tiles, ty, threads, smem = p
     assert 1 <= len(tiles) <= nsm
-    assert threads % 32 == 0 and (ty + 1) * (nx // 4) <= threads <= 416   # 416 x 152 registers fit an SM
+    assert threads % 32 == 0 and (ty + 1) * (nx // 4) <= threads <= 384   # 12 warps x 168 registers fit an SM
     na = 12 if lossy else 9
     xw = (2 * L + 3) // 4 * 4   # staged x-slab auxiliaries per row, padded to 16 bytes
     assert smem == ((3 * na * (ty + 1) + 6 + 6 * (ty + 1)) * nx + 3 * 4 * (ty + 1) * xw) * 4 <= SMEM_MAX

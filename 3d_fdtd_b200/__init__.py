@@ -182,6 +182,7 @@ SIGNATURES = {
     "fdtd_spline_store_unbind": (i, [C.c_void_p, T]),
     "fdtd_spline_store_gradient": (i, [C.c_void_p, d, dp, dp]),
     "fdtd_spline_store_gradient_exact": (i, [C.c_void_p, d, dp, dp]),
+    "fdtd_spline_store_gradient_step": (i, [C.c_void_p, d, d, dp]),
     "fdtd_spline_store_free": (None, [C.c_void_p]),
     "timefield3d_get_stream": (C.c_void_p, [T]),
     "timefield3d_upload_materials": (i, [T]),
@@ -189,6 +190,8 @@ SIGNATURES = {
     "timefield3d_set_wave_steps": (i, [T, i, i, i]),
     "fdtd_wave_schedule": (i, [i, i, i, i, i, i, i, ip, i, i, ip, i, ip]),
     "timefield3d_read_kernel_timing": (i, [T, dp, C.POINTER(ll)]),
+    "fdtd_sweep_run": (i, [C.POINTER(T), i, d, ip, i, i, d]),
+    "fdtd_sweep_barrier_selftest": (i, [d]),
     "fdtd_stream_plan": (i, [i, i, i, i, i, i, ip, i, ip, ip, C.POINTER(C.c_longlong)]),
     "fdtd_mode_overlap_plane_noalloc": (i, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, i, i, i, i, i,
                                             C.c_void_p, i, i, d, i, d, C.c_void_p, C.c_void_p]),

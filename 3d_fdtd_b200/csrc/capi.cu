@@ -1311,6 +1311,44 @@ complex fdtd_mode_solve_beta_squared(mode *psi, double omega, double tol, mode *
 
 int fdtd_mode_solve_restarts(void) { return last_mode_restarts; }
 
+int fdtd_sweep_run(const timefield3d *grids, int ngrids, double delta_t, const int *nsteps, int steps_per_launch,
+                   int band_rows, double tiles_per_sm)
+{
+    LOCK;
+    if (!grids || !nsteps || ngrids <= 0 || !(delta_t > 0) || !std::isfinite(delta_t)) {
+        set_error(FDTD_ERR_ARG, "fdtd_sweep_run: grids, nsteps, ngrids > 0 and a positive delta_t are required");
+        return FDTD_ERR_ARG;
+    }
+    std::vector<Grid *> gs;
+    std::vector<int> ns(nsteps, nsteps + ngrids);
+    for (int i = 0; i < ngrids; i++) {
+        Grid *g = dev_grid(grids[i]);
+        if (!g) return fdtd_last_error() ? fdtd_last_error() : FDTD_ERR_ARG;
+        gs.push_back(g);
+    }
+    TraceRange tr("fdtd_sweep_run");
+    if (!run_sweep(gs, delta_t, ns, steps_per_launch, band_rows, tiles_per_sm)) return fdtd_last_error();
+    return FDTD_OK;
+}
+
+int fdtd_sweep_barrier_selftest(double limit_seconds)
+{
+    LOCK;
+    if (!device_available()) return fdtd_last_error();
+    if (!(limit_seconds > 0.0) || limit_seconds > 10.0) {
+        set_error(FDTD_ERR_ARG, "sweep barrier self-test limit %g s: must be in (0, 10]", limit_seconds);
+        return FDTD_ERR_ARG;
+    }
+    int timed_out = 0;
+    if (!sweep_barrier_selftest((unsigned long long)(limit_seconds * 1e9), &timed_out)) return fdtd_last_error();
+    if (!timed_out) {
+        set_error(FDTD_ERR_CUDA, "sweep barrier self-test: the wait completed although nothing could complete it");
+        return FDTD_ERR_CUDA;
+    }
+    set_error(FDTD_ERR_TIMEOUT, "sweep barrier self-test: the bounded wait gave up as designed");
+    return FDTD_ERR_TIMEOUT;
+}
+
 int fdtd_wait_selftest(double limit_seconds, double *elapsed_seconds)
 {
     LOCK;

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <unordered_map>
 
@@ -1321,6 +1322,158 @@ bool drain_kernel_timing(Grid *g, int set)
 }
 
 static bool run_steps_in(Grid *g, double dt, int nsteps);
+
+// ============================================================================
+// candidate sweeps: many grids in persistent launches (yee_sweep.cu)
+// ============================================================================
+bool run_sweep(const std::vector<Grid *> &gs, double dt, const std::vector<int> &nsteps, int steps_per_launch,
+               int ty_cap, double tiles_per_sm)
+{
+    const int ng = (int)gs.size();
+    if (ng <= 0 || (int)nsteps.size() != ng || steps_per_launch < 1 || steps_per_launch > 4096 || ty_cap < 0 ||
+        !(tiles_per_sm > 0) || tiles_per_sm > 16) {
+        set_error(FDTD_ERR_ARG, "sweep: no grids, or steps_per_launch not in [1, 4096], ty_cap < 0, or tiles_per_sm "
+                                "not in (0, 16]");
+        return false;
+    }
+    int nsm = 0;
+    if (!sweep_setup(&nsm)) return false;
+    const Grid *g0 = gs[0];
+    const int L0 = g0->boundary == FDTD_BOUNDARY_CPML ? g0->L : 0;
+    for (int i = 0; i < ng; i++) {
+        Grid *g = gs[i];
+        for (int k = 0; k < i; k++)
+            if (gs[k] == g) {
+                set_error(FDTD_ERR_ARG, "sweep: grid %d appears twice", i);
+                return false;
+            }
+        const int L = g->boundary == FDTD_BOUNDARY_CPML ? g->L : 0;
+        if (nsteps[i] < 0 || !fast32_path(g) || L != L0 || g->sig_e != g0->sig_e || !g->probes.empty() ||
+            !g->binds.empty() || !stream_supported(g->nx, g->ny, g->nz, g->sig_e, L)) {
+            set_error(FDTD_ERR_UNSUPPORTED,
+                      "sweep: grid %d must be FP32 with a CPML (or PEC walls) like grid 0, the same loss, no probes or "
+                      "bound tapers, nx a multiple of 4, and nsteps >= 0",
+                      i);
+            return false;
+        }
+    }
+    // every grid on the one-pass path (two field and auxiliary sets), prepared
+    // as for timefield3d_run; the first step's scheduled source written
+    cudaStream_t sst = sweep_stream();
+    for (Grid *g : gs) {
+        if (g->yee_variant != FDTD_YEE_STREAM) {
+            g->yee_variant = FDTD_YEE_STREAM;
+            g->pp_synced = false;
+            g->version++;
+        }
+        if (!prepare_run(g, dt)) return false;
+        if (g->sched.active && !enqueue_schedule(g, 0)) return false;
+        CK(cudaEventRecord(g->ev_fork, g->st));
+        CK(cudaStreamWaitEvent(sst, g->ev_fork, 0));
+    }
+    // tile plans: each grid's share of nsm * tiles_per_sm tiles in proportion to its cells
+    double total = 0;
+    for (Grid *g : gs) total += (double)g->n;
+    std::vector<StreamPlan> plans(ng);
+    int threads = 0;
+    size_t smem = 0, ntile = 0, npart = 0;
+    std::vector<size_t> toff(ng), poff(ng);
+    std::vector<int> nparts(ng);
+    for (int i = 0; i < ng; i++) {
+        Grid *g = gs[i];
+        const int share = std::max(1, (int)std::lround(nsm * tiles_per_sm * (double)g->n / total));
+        if (!stream_plan(g->nx, g->ny, g->nz, L0, g->sig_e, share, &plans[i], ty_cap)) {
+            set_error(FDTD_ERR_UNSUPPORTED, "sweep: no tile plan for grid %d", i);
+            return false;
+        }
+        threads = std::max(threads, plans[i].threads);
+        smem = std::max(smem, plans[i].smem);
+        toff[i] = ntile;
+        ntile += plans[i].tiles.size();
+        nparts[i] = g->njobs > 0 ? overlap_parts(g->job_cells) : 0;
+        poff[i] = npart;
+        npart += 2 * (size_t)g->njobs * nparts[i];
+    }
+    StreamTile **dt_tiles = sweep_tiles(ntile * sizeof(StreamTile));
+    double2 **dt_parts = sweep_partials(std::max<size_t>(npart, 1) * sizeof(double2));
+    if (!dt_tiles || !dt_parts) return false;
+    std::vector<StreamTile> all;
+    for (auto &p : plans) all.insert(all.end(), p.tiles.begin(), p.tiles.end());
+    CK(cudaStreamSynchronize(sst));   // the previous sweep no longer reads the tables
+    CK(cudaMemcpyAsync(*dt_tiles, all.data(), all.size() * sizeof(StreamTile), cudaMemcpyHostToDevice, sst));
+    // per grid, the launch-independent part of its entry
+    std::vector<SweepGrid> proto(ng);
+    for (int i = 0; i < ng; i++) {
+        Grid *g = gs[i];
+        SweepGrid &e = proto[i];
+        e = SweepGrid{};
+        for (int p = 0; p < 2; p++) {
+            StreamArgs &a = e.args[p];
+            a.nx = g->nx; a.ny = g->ny; a.nz = g->nz; a.L = L0; a.ty = plans[i].ty;
+            for (int m = 0; m < 6; m++) { a.f_in[m] = (const float *)g->f[p][m]; a.f_out[m] = (float *)g->f[1 - p][m]; }
+            for (int c = 0; c < 3; c++) { a.cb[c] = g->cb[c]; a.ca[c] = g->sig_e ? g->ca[c] : nullptr; }
+            a.hb = (float)(dt / g->dx);
+            a.dx = (float)g->dx;
+            for (int ax = 0; ax < 3; ax++) {
+                for (int w = 0; w < 4; w++) {
+                    a.psi_in[ax][w] = (const float *)g->psi[p][ax][w];
+                    a.psi_out[ax][w] = (float *)g->psi[1 - p][ax][w];
+                }
+                for (int w = 0; w < 6; w++) a.prof[w][ax] = (const float *)g->prof[w][ax];
+            }
+            a.src = source_table(g);
+            a.tiles = *dt_tiles + toff[i];
+            e.fout[p] = (const float *const *)g->d_fptr[1 - p];
+        }
+        e.ntiles = (int)plans[i].tiles.size();
+        e.nx = g->nx; e.ny = g->ny;
+        e.jobs = g->d_jobs;
+        e.njobs = g->njobs;
+        e.nparts = nparts[i];
+        e.partials = *dt_parts + poff[i];
+        e.scale = -0.5 * g->dx * g->dx;
+        e.dt = dt;
+        e.step = g->d_step;
+        if (g->sched.active) {
+            if (!schedule_job(g, &e.src)) return false;
+            e.src.win = mode_window(e.src.nx, e.src.ny, e.src.cx, e.src.cy, e.src.mi, e.src.mj, e.src.ratio);
+            const long long cells = (long long)e.src.win.wni * e.src.win.wnj;
+            e.src_warps = (int)std::max<long long>(1, std::min<long long>((cells + 31) / 32, 4 * 384));
+        }
+    }
+    // launches of steps_per_launch steps until every grid has run its own count
+    const int most = *std::max_element(nsteps.begin(), nsteps.end());
+    std::vector<std::vector<SweepGrid>> launches;
+    std::vector<int> lsteps;
+    for (int l0 = 0; l0 < most; l0 += steps_per_launch) {
+        std::vector<SweepGrid> row(proto);
+        int lmax = 0;
+        for (int i = 0; i < ng; i++) {
+            row[i].steps = std::max(0, std::min(steps_per_launch, nsteps[i] - l0));
+            row[i].base = gs[i]->host_steps + std::min(l0, nsteps[i]);
+            row[i].p0 = (gs[i]->cur + std::min(l0, nsteps[i])) & 1;
+            lmax = std::max(lmax, row[i].steps);
+        }
+        launches.push_back(std::move(row));
+        lsteps.push_back(lmax);
+    }
+    if (!launches.empty() &&
+        !sweep_launch(launches, lsteps, L0 > 0, g0->sig_e, threads, smem, 1000000000ull))
+        return false;
+    // the grids' own streams continue after the sweep
+    CK(cudaEventRecord(sweep_event(), sst));
+    for (int i = 0; i < ng; i++) {
+        Grid *g = gs[i];
+        CK(cudaStreamWaitEvent(g->st, sweep_event(), 0));
+        launch_sweep_err_to_grid(sweep_err(), g->d_err, g->st);
+        g->cur = (g->cur + nsteps[i]) & 1;
+        g->host_steps += nsteps[i];
+        // as after timefield3d_run, the plane holds the last step's source
+        if (g->sched.active && nsteps[i] > 0 && !enqueue_schedule(g, -1)) return false;
+    }
+    CKL("sweep");
+    return true;
+}
 
 bool run_steps(Grid *g, double dt, int nsteps)
 {

@@ -237,6 +237,8 @@ struct TraceRange {
 bool enqueue_step(Grid *g, double dt, bool with_extras);
 bool enqueue_after_step(Grid *g, double dt);
 bool run_steps(Grid *g, double dt, int nsteps);
+bool run_sweep(const std::vector<Grid *> &gs, double dt, const std::vector<int> &nsteps, int steps_per_launch,
+               int ty_cap, double tiles_per_sm);
 bool drain_kernel_timing(Grid *g, int set);
 bool rebuild_jobs(Grid *g);
 

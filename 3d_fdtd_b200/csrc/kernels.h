@@ -210,16 +210,55 @@ struct StreamArgs {
     SourcePlanes src;
     const StreamTile *tiles;
 };
-constexpr size_t kStreamSmemBudget = 232448;   // dynamic shared memory per block, sm_100 maximum
+constexpr size_t kStreamSmemBudget = 231424;   // dynamic shared memory per block: the sm_100 maximum less 1 KB of static room
 // staged x-slab auxiliaries per row: 2L, padded to 16 bytes
 __host__ __device__ inline int stream_xpsi_stride(int L) { return (2 * L + 3) & ~3; }
 int stream_supported(int nx, int ny, int nz, bool lossy, int L);
-// tiles for a grid on a device with nsm SMs; false when the grid cannot use the kernel
-bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan *out);
+// tiles for a grid over nsm blocks (one per SM); ty_cap > 0 caps the rows of a
+// band (the autotuner's tile-shape knob); false when the grid cannot use the kernel
+bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan *out, int ty_cap = 0);
 // allow `smem` bytes of dynamic shared memory for every instantiation and check
 // that blocks of `threads` threads can launch (host, not stream-ordered)
 bool stream_configure(size_t smem, int threads);
 void launch_yee_stream(const StreamArgs &a, const StreamPlan &p, cudaStream_t st);
+
+// yee_sweep.cu: many grids advanced together by persistent launches of S
+// steps (see the file's header); one entry per grid per launch
+struct SweepGrid {
+    StreamArgs args[2];          // input set p (output 1 - p); args[p].tiles = this grid's sweep tiles
+    int ntiles;
+    const float *const *fout[2]; // field pointers of the output set when the input is set p
+    int nx, ny;
+    const OverlapJob *jobs;
+    int njobs, nparts;
+    double2 *partials;           // [2][njobs * nparts], by step parity
+    double scale, dt;
+    SourceJob src;               // plane null: no scheduled source
+    int src_warps;
+    long long base;              // steps taken when the launch starts
+    long long *step;             // the grid's device step counter
+    int p0;                      // input set of the grid's first step in the launch
+    int steps;                   // steps of this grid in the launch (0: idle)
+};
+
+struct SweepArgs {
+    const SweepGrid *grids;
+    int ngrids, steps;           // steps: the most of any grid
+    unsigned *bar;               // barrier arrivals, zero when the launch starts
+    int *err;                    // set when a barrier wait gives up
+    unsigned long long wait_ns;
+    unsigned arrivals;           // arrivals per barrier (the grid size)
+};
+bool sweep_setup(int *nsm);
+cudaStream_t sweep_stream();
+cudaEvent_t sweep_event();
+int *sweep_err();
+StreamTile **sweep_tiles(size_t bytes);     // grown device buffers owned by the sweep
+double2 **sweep_partials(size_t bytes);
+bool sweep_launch(const std::vector<std::vector<SweepGrid>> &launches, const std::vector<int> &steps, bool cpml,
+                  bool lossy, int threads, size_t smem, unsigned long long wait_ns);
+void launch_sweep_err_to_grid(const int *sweep, int *grid, cudaStream_t st);
+bool sweep_barrier_selftest(unsigned long long limit_ns, int *timed_out);
 
 // yee_wave.cu: S steps of the flat4 update in one persistent, cooperative
 // launch, wavefront-ordered in z (see the file's header)

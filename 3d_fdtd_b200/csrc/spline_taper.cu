@@ -182,6 +182,13 @@ template <typename P> void dfree(P *&p)
     p = nullptr;
 }
 
+// store cell of plane k, row j, edge e (0 right, 1 left), offset d in -1..1
+// from the cell holding the edge
+inline size_t store_cell(int height, int k, int j, int e, int d)
+{
+    return ((size_t)(j + (size_t)height * k) * 2 + e) * 3 + (d + 1);
+}
+
 // the spline edge store: a TaperDev (same store / gradient kernels as the
 // reference tapers) keyed by this object, cells [k][j][edge], edge 0 right
 struct SplineStore {
@@ -203,7 +210,7 @@ bool store_prepare(SplineStore *s, Grid *g)
     if (!grid_ensure_device(g)) return false;
     TaperDev *td = taper_lookup(store_key(s), true);
     const int height = s->sg.top - s->sg.bottom, length = s->sg.end_z - s->sg.start_z;
-    const int ncell = 2 * height * length;
+    const int ncell = 6 * height * length;   // per (k, j, edge): the edge cell and its two x neighbours
     if (td->ncell != ncell || td->duration != s->duration || td->prec != g->prec) {
         cudaDeviceSynchronize();
         dfree(td->d_fwd); dfree(td->d_adj); dfree(td->d_cells); dfree(td->d_grad);
@@ -225,10 +232,12 @@ bool store_prepare(SplineStore *s, Grid *g)
             for (int j = 0; j < height; j++)
                 for (int e = 0; e < 2; e++) {
                     const double x = e == 0 ? s->sg.xr[k] : s->sg.xl[k];
-                    int i = (int)std::floor(x);
-                    i = std::max(0, std::min(g->nx - 1, i));
-                    s->cells[e + 2 * (j + (size_t)height * k)] =
-                        i + (long long)g->nx * ((s->sg.bottom + j) + (long long)g->ny * (s->sg.start_z + k));
+                    for (int d = -1; d <= 1; d++) {
+                        int i = (int)std::floor(x) + d;
+                        i = std::max(0, std::min(g->nx - 1, i));
+                        s->cells[store_cell(height, k, j, e, d)] =
+                            i + (long long)g->nx * ((s->sg.bottom + j) + (long long)g->ny * (s->sg.start_z + k));
+                    }
                 }
         if (!cuda_ok(cudaStreamSynchronize(g->st), "sync") ||
             !cuda_ok(cudaMemcpy(td->d_cells, s->cells.data(), ncell * sizeof(long long), cudaMemcpyHostToDevice),
@@ -372,28 +381,11 @@ int fdtd_spline_store_unbind(fdtd_spline_store store, timefield3d psi)
     return FDTD_OK;
 }
 
-static int spline_gradient(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient, bool exact);
-
-int fdtd_spline_store_gradient(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient)
+// g of every stored cell (FP64 sums on the device): the reference's field
+// product (exact = false) or the exact adjoint's (exact = true)
+static bool cell_gradients(TaperDev *td, bool exact, std::vector<double> &gcell)
 {
-    return spline_gradient(store, ep_diff, grad, cell_gradient, false);
-}
-
-int fdtd_spline_store_gradient_exact(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient)
-{
-    return spline_gradient(store, ep_diff, grad, cell_gradient, true);
-}
-
-static int spline_gradient(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient, bool exact)
-{
-    std::lock_guard<std::mutex> lock(api_mutex());
-    auto *s = (SplineStore *)store;
-    TaperDev *td = store_known(s) ? taper_lookup(store_key(s), false) : nullptr;
-    if (!td || !td->d_fwd || !grad) {
-        set_error(FDTD_ERR_ARG, "fdtd_spline_store_gradient: no stored fields for this store");
-        return FDTD_ERR_ARG;
-    }
-    if (!cuda_ok(cudaDeviceSynchronize(), "sync")) return fdtd_last_error();
+    if (!cuda_ok(cudaDeviceSynchronize(), "sync")) return false;
     if (exact && td->prec == FDTD_F64)
         launch_ep_gradient_exact<double>((const double *)td->d_fwd, (const double *)td->d_adj, td->ncell,
                                          td->duration, td->d_grad, 0);
@@ -406,11 +398,32 @@ static int spline_gradient(fdtd_spline_store store, double ep_diff, double *grad
     else
         launch_ep_gradient<float>((const float *)td->d_fwd, (const float *)td->d_adj, td->ncell, td->duration,
                                   td->d_grad, 0);
-    if (!cuda_ok(cudaGetLastError(), "ep gradient")) return fdtd_last_error();
-    std::vector<double> gcell(td->ncell);
-    if (!cuda_ok(cudaMemcpy(gcell.data(), td->d_grad, td->ncell * sizeof(double), cudaMemcpyDeviceToHost),
-                 "gradient D2H"))
-        return fdtd_last_error();
+    if (!cuda_ok(cudaGetLastError(), "ep gradient")) return false;
+    gcell.assign(td->ncell, 0.0);
+    return cuda_ok(cudaMemcpy(gcell.data(), td->d_grad, td->ncell * sizeof(double), cudaMemcpyDeviceToHost),
+                   "gradient D2H");
+}
+
+static TaperDev *store_dev(SplineStore *s, const double *grad)
+{
+    TaperDev *td = store_known(s) ? taper_lookup(store_key(s), false) : nullptr;
+    if (!td || !td->d_fwd || !grad) {
+        set_error(FDTD_ERR_ARG, "spline store gradient: no stored fields for this store");
+        return nullptr;
+    }
+    return td;
+}
+
+// d/dw_c of the core: the edge cell's fill fraction moves by 1/(2 disc) per um
+// of width on both edges (timefield3d_set_spline_taper's fill rule)
+static int spline_gradient(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient, bool exact)
+{
+    std::lock_guard<std::mutex> lock(api_mutex());
+    auto *s = (SplineStore *)store;
+    TaperDev *td = store_dev(s, grad);
+    if (!td) return FDTD_ERR_ARG;
+    std::vector<double> gcell;
+    if (!cell_gradients(td, exact, gcell)) return fdtd_last_error();
     if (cell_gradient) std::copy(gcell.begin(), gcell.end(), cell_gradient);
     const SplineGeom &sg = s->sg;
     const int height = sg.top - sg.bottom, length = sg.end_z - sg.start_z;
@@ -418,10 +431,70 @@ static int spline_gradient(fdtd_spline_store store, double ep_diff, double *grad
         double acc = 0.0;
         for (int k = 0; k < length; k++) {
             double row = 0.0;
-            for (int j = 0; j < height; j++) row += gcell[0 + 2 * (j + (size_t)height * k)] + gcell[1 + 2 * (j + (size_t)height * k)];
+            for (int j = 0; j < height; j++)
+                row += gcell[store_cell(height, k, j, 0, 0)] + gcell[store_cell(height, k, j, 1, 0)];
             acc += sg.W[(size_t)k * sg.K + c] * row;
         }
         grad[c] = acc * ep_diff / (2.0 * sg.disc);
+    }
+    return FDTD_OK;
+}
+
+int fdtd_spline_store_gradient(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient)
+{
+    return spline_gradient(store, ep_diff, grad, cell_gradient, false);
+}
+
+int fdtd_spline_store_gradient_exact(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient)
+{
+    return spline_gradient(store, ep_diff, grad, cell_gradient, true);
+}
+
+// fill fraction of cell i for a core [xl, xr) (the raster's rule, clamped)
+static double cover(int i, double xl, double xr)
+{
+    const double f = std::min((double)i + 1.0, xr) - std::max((double)i, xl);
+    return f <= 0.0 ? 0.0 : (f >= 1.0 ? 1.0 : f);
+}
+
+int fdtd_spline_store_gradient_step(fdtd_spline_store store, double ep_diff, double delta, double *grad)
+{
+    std::lock_guard<std::mutex> lock(api_mutex());
+    auto *s = (SplineStore *)store;
+    TaperDev *td = store_dev(s, grad);
+    if (!td) return FDTD_ERR_ARG;
+    const SplineGeom &sg = s->sg;
+    if (!(delta > 0) || delta / (2.0 * sg.disc) > 1.0) {
+        set_error(FDTD_ERR_ARG,
+                  "spline store step gradient: delta %g um must be positive and move an edge by at most one cell",
+                  delta);
+        return FDTD_ERR_ARG;
+    }
+    std::vector<double> gcell;
+    if (!cell_gradients(td, true, gcell)) return fdtd_last_error();
+    const int height = sg.top - sg.bottom, length = sg.end_z - sg.start_z;
+    for (int c = 0; c < sg.K; c++) {
+        double acc = 0.0;
+        for (int k = 0; k < length; k++) {
+            const double sh = delta * std::fabs(sg.W[(size_t)k * sg.K + c]) / (2.0 * sg.disc);   // edge shift, cells
+            const double sg_w = sg.W[(size_t)k * sg.K + c] >= 0 ? 1.0 : -1.0;
+            const double xl = sg.xl[k], xr = sg.xr[k];
+            const int base[2] = {(int)std::floor(xr), (int)std::floor(xl)};
+            double row = 0.0;
+            for (int e = 0; e < 2; e++)
+                for (int d = -1; d <= 1; d++) {
+                    const int i = base[e] + d;
+                    if (e == 1 && i >= base[0] - 1) continue;   // already counted with the right edge's cells
+                    // width + delta W (both edges out by sh when W >= 0) against width - delta W
+                    const double df = sg_w * (cover(i, xl - sh, xr + sh) - cover(i, xl + sh, xr - sh));
+                    if (df == 0.0) continue;
+                    double gs = 0.0;
+                    for (int j = 0; j < height; j++) gs += gcell[store_cell(height, k, j, e, d)];
+                    row += gs * df;
+                }
+            acc += row;
+        }
+        grad[c] = acc * ep_diff / (2.0 * delta);
     }
     return FDTD_OK;
 }

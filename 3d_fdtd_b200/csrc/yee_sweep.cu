@@ -1,0 +1,366 @@
+// yee_sweep.cu -- many grids (taper candidates of uneven length) advanced
+// together by one persistent launch per chunk of steps.
+//
+// The reference simulates one design at a time (3d_fdtd.c:93-202).  An
+// optimisation sweep runs many independent candidates; here every resident
+// candidate advances inside ONE cooperative launch of S steps (one block per
+// SM, all co-resident), each candidate for at most its own remaining steps.
+// Per step, three phases separated by grid barriers where needed:
+//   A  the one-pass FP32 Yee update (yee_stream.cu) of every candidate still
+//      running: its (band, chunk) tiles, dealt round robin over the blocks;
+//   -- barrier --
+//   B  each candidate's step tail: the overlap partials of its monitors (one
+//      warp per partial, the same partial as the per-step tail's 256-thread
+//      block) and its scheduled source plane for the next step;
+//   -- barrier --
+//   C  the monitors of the step: partials added in order, accumulated per
+//      frequency with Kahan compensation at step base + s (one warp per
+//      monitor).  Partials are double-buffered by step parity, so phase C of
+//      step s runs beside phase A of step s+1 without a barrier between them.
+// Every candidate's fields, auxiliaries and monitors are those of the same
+// candidate run alone with FDTD_YEE_STREAM, bit for bit: the tile split does
+// not change any cell's arithmetic and the reductions keep their order.
+//
+// Memory: loads of data written inside the launch (fields through the
+// L2-only cp.async path, CPML auxiliaries, source planes, partials) are
+// coherent; every grid barrier is arrival (release) then a bounded poll
+// (acquire).  A barrier that waits longer than its limit sets the sweep's
+// error flag; the flag stops every later wait, the launch ends, and the grids
+// report FDTD_ERR_TIMEOUT at their next synchronising call.
+#include "stream_cells.cuh"
+#include "plane_ops.cuh"
+#include "engine.h"
+
+#define CK_RET(call)                               \
+    do {                                           \
+        if (!cuda_ok((call), #call)) return false; \
+    } while (0)
+
+namespace fdtd {
+
+__device__ __forceinline__ unsigned long long sweep_clock()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ int ld_relaxed_i32(const int *p)
+{
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// grid barrier number k (1, 2, ...): every block arrives once; true when all
+// a.arrivals arrived, false when the wait gave up (or another block's did)
+__device__ bool sweep_barrier(const SweepArgs &a, unsigned k, int *abort_s)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ab = 0;
+        __threadfence();
+        atomicAdd(a.bar, 1u);
+        const unsigned target = k * a.arrivals;
+        unsigned long long t0 = 0;
+        unsigned ns = 32;
+        for (;;) {
+            if (ld_acquire_u32(a.bar) >= target) break;
+            if (ld_relaxed_i32(a.err) != 0) {
+                ab = 1;
+                break;
+            }
+            const unsigned long long now = sweep_clock();
+            if (t0 == 0) {
+                t0 = now;
+            } else if (now - t0 > a.wait_ns) {
+                atomicCAS(a.err, 0, 1);
+                ab = 1;
+                break;
+            }
+            __nanosleep(ns);
+            if (ns < 256) ns <<= 1;
+        }
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        *abort_s = ab;
+    }
+    __syncthreads();
+    return *abort_s == 0;
+}
+
+template <bool CPML, bool LOSSY>
+__global__ void __launch_bounds__(kStreamMaxThreads, 1) k_sweep(SweepArgs a)
+{
+    extern __shared__ __align__(16) float sm[];
+    __shared__ int abort_s;
+    const int G = gridDim.x, warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * warps + warp, nw = G * warps;
+    unsigned nbar = 0;
+    for (int s = 0; s < a.steps; s++) {
+        // ---- A: Yee tiles of the running grids, round robin over the blocks
+        int item = 0;
+        for (int g = 0; g < a.ngrids; g++) {
+            const SweepGrid &sg = a.grids[g];
+            if (s >= sg.steps) continue;
+            const int first = (blockIdx.x - item % G + G) % G;   // this block's first tile of the grid
+            for (int t = first; t < sg.ntiles; t += G) {
+                __syncthreads();   // the block's previous tile no longer reads shared memory
+                const StreamArgs &sa = sg.args[(sg.p0 + s) & 1];
+                stream_tile<CPML, LOSSY, true>(sa, sa.tiles[t], sm);
+            }
+            item += sg.ntiles;
+        }
+        if (!sweep_barrier(a, ++nbar, &abort_s)) return;
+        // ---- B: overlap partials of step s, scheduled source of step s+1
+        int w = 0;
+        for (int g = 0; g < a.ngrids; g++) {
+            const SweepGrid &sg = a.grids[g];
+            if (s >= sg.steps) continue;
+            const int nov = sg.njobs * sg.nparts;
+            const float *const *f = sg.fout[(sg.p0 + s) & 1];
+            for (int i = (gw - w % nw + nw) % nw; i < nov; i += nw) {
+                const int jid = i / sg.nparts, part = i - jid * sg.nparts;
+                overlap_warp<float>(f, sg.nx, sg.ny, sg.jobs[jid], part, sg.nparts,
+                                    sg.partials + (size_t)(s & 1) * nov + i);
+            }
+            w += nov;
+            if (sg.src.plane) {
+                const SrcStep v = schedule_step(sg.src, sg.base + s + 1);
+                for (int i = (gw - w % nw + nw) % nw; i < sg.src_warps; i += nw)
+                    mode_source_cells(sg.src, (long long)i * 32 + lane, (long long)sg.src_warps * 32, v);
+                w += sg.src_warps;
+            }
+        }
+        if (!sweep_barrier(a, ++nbar, &abort_s)) return;
+        // ---- C: the monitors of step s (no barrier after: the partials of the
+        //      next step go to the other buffer)
+        w = 0;
+        for (int g = 0; g < a.ngrids; g++) {
+            const SweepGrid &sg = a.grids[g];
+            if (s >= sg.steps) continue;
+            const int nov = sg.njobs * sg.nparts;
+            for (int jid = (gw - w % nw + nw) % nw; jid < sg.njobs; jid += nw) {
+                const double2 *pp = sg.partials + (size_t)(s & 1) * nov + (size_t)jid * sg.nparts;
+                double sre = 0.0, sim = 0.0;
+                for (int p = 0; p < sg.nparts; p++) {
+                    const double2 v = pp[p];
+                    sre = dadd(sre, v.x);
+                    sim = dadd(sim, v.y);
+                }
+                const double2 tot = make_double2(dmul(sg.scale, sre), dmul(sg.scale, sim));
+                const OverlapJob jb = sg.jobs[jid];
+                if (jb.inst && lane == 0) *jb.inst = tot;
+                if (jb.acc)
+                    for (int f = lane; f < jb.nfreq; f += 32) accumulate_frequency(jb, f, tot, sg.dt, sg.base + s);
+            }
+            w += sg.njobs;
+        }
+    }
+    // device step counters: the block that owns each grid's last monitor work
+    // is irrelevant here; block 0 writes them once every phase C is issued
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        for (int g = 0; g < a.ngrids; g++) *a.grids[g].step = a.grids[g].base + a.grids[g].steps;
+}
+
+// a timed-out sweep marks every grid it ran (their next synchronising call
+// reports FDTD_ERR_TIMEOUT)
+__global__ void k_sweep_err_to_grid(const int *sweep, int *grid)
+{
+    if (*sweep) *grid = 1;
+}
+
+void launch_sweep_err_to_grid(const int *sweep, int *grid, cudaStream_t st)
+{
+    note_launch(1);
+    k_sweep_err_to_grid<<<1, 1, 0, st>>>(sweep, grid);
+}
+
+// A barrier that nothing completes (arrivals one more than the grid): every
+// block's wait gives up after the limit and the flag is set.
+__global__ void k_sweep_barrier_selftest(SweepArgs a)
+{
+    __shared__ int abort_s;
+    sweep_barrier(a, 1, &abort_s);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+namespace {
+
+struct SweepContext {
+    cudaStream_t st = nullptr;
+    int dev = -1, nsm = 0;
+    unsigned *d_bar = nullptr;
+    int *d_err = nullptr;
+    SweepGrid *d_grids = nullptr;
+    size_t grids_cap = 0;
+    StreamTile *d_tiles = nullptr;
+    size_t tiles_cap = 0;
+    double2 *d_partials = nullptr;
+    size_t partials_cap = 0;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev = nullptr;
+};
+
+SweepContext &ctx()
+{
+    static SweepContext c;
+    return c;
+}
+
+template <typename P> bool grow(P **p, size_t &cap, size_t need)
+{
+    if (*p && cap >= need) return true;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    cap = 0;
+    if (!cuda_ok(cudaMalloc((void **)p, need ? need : 16), "cudaMalloc(sweep)")) return false;
+    cap = need;
+    return true;
+}
+
+}  // namespace
+
+template <bool CPML, bool LOSSY> static const void *sweep_kernel() { return (const void *)k_sweep<CPML, LOSSY>; }
+
+bool sweep_setup(int *nsm_out)
+{
+    SweepContext &c = ctx();
+    int dev = 0;
+    CK_RET(cudaGetDevice(&dev));
+    if (c.dev != dev) {
+        if (c.st) cudaStreamDestroy(c.st);
+        c = SweepContext{};
+        c.dev = dev;
+        CK_RET(cudaDeviceGetAttribute(&c.nsm, cudaDevAttrMultiProcessorCount, dev));
+        CK_RET(cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking));
+        CK_RET(cudaEventCreateWithFlags(&c.ev, cudaEventDisableTiming));
+        CK_RET(cudaMalloc(&c.d_bar, sizeof(unsigned)));
+        CK_RET(cudaMalloc(&c.d_err, sizeof(int)));
+        CK_RET(cudaMemset(c.d_err, 0, sizeof(int)));
+    }
+    *nsm_out = c.nsm;
+    return true;
+}
+
+// Runs the launches described by `launches` (each a list of SweepGrid, one per
+// grid) on the sweep stream as one captured graph.  Tile tables and partial
+// buffers are the caller's (already uploaded to `tiles`/`partials`).
+bool sweep_launch(const std::vector<std::vector<SweepGrid>> &launches, const std::vector<int> &steps, bool cpml,
+                  bool lossy, int threads, size_t smem, unsigned long long wait_ns)
+{
+    SweepContext &c = ctx();
+    const int ng = launches.empty() ? 0 : (int)launches[0].size();
+    const size_t per = (size_t)ng;
+    std::vector<SweepGrid> flat;
+    for (auto &l : launches) flat.insert(flat.end(), l.begin(), l.end());
+    CK_RET(cudaStreamSynchronize(c.st));
+    CK_RET(cudaMemsetAsync(c.d_err, 0, sizeof(int), c.st));
+    if (c.exec) {
+        cudaGraphExecDestroy(c.exec);
+        c.exec = nullptr;
+    }
+    if (!grow(&c.d_grids, c.grids_cap, flat.size() * sizeof(SweepGrid))) return false;
+    CK_RET(cudaMemcpyAsync(c.d_grids, flat.data(), flat.size() * sizeof(SweepGrid), cudaMemcpyHostToDevice, c.st));
+    const void *fn = cpml ? (lossy ? sweep_kernel<true, true>() : sweep_kernel<true, false>())
+                          : (lossy ? sweep_kernel<false, true>() : sweep_kernel<false, false>());
+    CK_RET(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CK_RET(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+    if (per_sm < 1) {
+        set_error(FDTD_ERR_CUDA, "sweep: a block of %d threads with %zu bytes of shared memory cannot be resident",
+                  threads, smem);
+        return false;
+    }
+    cudaGraph_t gr;
+    CK_RET(cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal));
+    bool ok = true;
+    for (size_t l = 0; l < launches.size() && ok; l++) {
+        SweepArgs a{};
+        a.grids = c.d_grids + l * per;
+        a.ngrids = ng;
+        a.steps = steps[l];
+        a.bar = c.d_bar;
+        a.err = c.d_err;
+        a.wait_ns = wait_ns;
+        a.arrivals = (unsigned)c.nsm;
+        ok = cudaMemsetAsync(c.d_bar, 0, sizeof(unsigned), c.st) == cudaSuccess;
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3((unsigned)c.nsm);
+        cfg.blockDim = dim3((unsigned)threads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = c.st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        note_launch(1);
+        if (ok) {
+            if (cpml && lossy) ok = cudaLaunchKernelEx(&cfg, k_sweep<true, true>, a) == cudaSuccess;
+            else if (cpml) ok = cudaLaunchKernelEx(&cfg, k_sweep<true, false>, a) == cudaSuccess;
+            else if (lossy) ok = cudaLaunchKernelEx(&cfg, k_sweep<false, true>, a) == cudaSuccess;
+            else ok = cudaLaunchKernelEx(&cfg, k_sweep<false, false>, a) == cudaSuccess;
+        }
+    }
+    cudaError_t ce = cudaStreamEndCapture(c.st, &gr);
+    if (!ok) {
+        if (ce == cudaSuccess) cudaGraphDestroy(gr);
+        return cuda_ok(cudaGetLastError(), "sweep capture") && false;
+    }
+    CK_RET(ce);
+    cudaError_t ie = cudaGraphInstantiate(&c.exec, gr, 0);
+    cudaGraphDestroy(gr);
+    CK_RET(ie);
+    CK_RET(cudaGraphLaunch(c.exec, c.st));
+    return true;
+}
+
+cudaStream_t sweep_stream() { return ctx().st; }
+cudaEvent_t sweep_event() { return ctx().ev; }
+int *sweep_err() { return ctx().d_err; }
+StreamTile **sweep_tiles(size_t need)
+{
+    SweepContext &c = ctx();
+    if (!grow(&c.d_tiles, c.tiles_cap, need)) return nullptr;
+    return &c.d_tiles;
+}
+double2 **sweep_partials(size_t need)
+{
+    SweepContext &c = ctx();
+    if (!grow(&c.d_partials, c.partials_cap, need)) return nullptr;
+    return &c.d_partials;
+}
+
+bool sweep_barrier_selftest(unsigned long long limit_ns, int *timed_out)
+{
+    int nsm = 0;
+    if (!sweep_setup(&nsm)) return false;
+    SweepContext &c = ctx();
+    CK_RET(cudaMemsetAsync(c.d_bar, 0, sizeof(unsigned), c.st));
+    int *d_err = nullptr;
+    CK_RET(cudaMalloc(&d_err, sizeof(int)));
+    CK_RET(cudaMemsetAsync(d_err, 0, sizeof(int), c.st));
+    SweepArgs a{};
+    a.bar = c.d_bar;
+    a.err = d_err;
+    a.wait_ns = limit_ns;
+    a.arrivals = 2;   // one block, two arrivals expected: never complete
+    note_launch(1);
+    k_sweep_barrier_selftest<<<1, 32, 0, c.st>>>(a);
+    bool ok = cuda_ok(cudaGetLastError(), "sweep barrier self-test") &&
+              cuda_ok(cudaMemcpyAsync(timed_out, d_err, sizeof(int), cudaMemcpyDeviceToHost, c.st), "D2H") &&
+              cuda_ok(cudaStreamSynchronize(c.st), "sync");
+    cudaFree(d_err);
+    return ok;
+}
+
+}  // namespace fdtd

@@ -381,7 +381,9 @@ int fdtd_spline_basis(int ncontrol, int start_z, int end_z, double *weights);
 int timefield3d_set_spline_taper(timefield3d psi, double ep, double mu, int ncontrol, const double *widths,
                                  double center_x, int start_z, int end_z, int bottom, int top);
 /* Edge store for the adjoint gradient of a spline taper: E at the cell holding
- * each core edge, per row and plane ([k][j][edge], edge 0 right, 1 left), for
+ * each core edge and at its two x neighbours, per row and plane
+ * ([k][j][edge][3], edge 0 right, 1 left; cells floor(x)-1, floor(x),
+ * floor(x)+1), for
  * `duration` steps, forward and adjoint, on the GPU.  Bind it to a grid like
  * adjoint3d_taper_bind_store (which 0 forward / 1 adjoint; after step n of
  * timefield3d_run it stores at t0 + dir*n); unbind before freeing. */
@@ -392,7 +394,7 @@ int fdtd_spline_store_bind(fdtd_spline_store store, timefield3d psi, int which, 
 int fdtd_spline_store_unbind(fdtd_spline_store store, timefield3d psi);
 /* grad[c] = sum_k sum_j W[k][c] / (2 disc) (g_right + g_left) ep_diff with
  * g = sum_t sum_m E_fwd E_adj at the edge cells; cell_gradient (optional,
- * 2*(top-bottom)*(end_z-start_z) values) receives g */
+ * 6*(top-bottom)*(end_z-start_z) values, the store's cell order) receives g */
 int fdtd_spline_store_gradient(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient);
 /* dF/d(control width) for a forward store (which 0, t0 0, dir 1) and an adjoint
  * store from timefield3d_set_exact_adjoint_schedule: per edge cell
@@ -401,6 +403,14 @@ int fdtd_spline_store_gradient(fdtd_spline_store store, double ep_diff, double *
  * omitted constant: the derivative of the simulated objective.  No reference
  * counterpart (generalises adjoint3d.c:339-418). */
 int fdtd_spline_store_gradient_exact(fdtd_spline_store store, double ep_diff, double *grad, double *cell_gradient);
+/* The same adjoint fields applied to a finite step: grad[c] = sum over the
+ * stored cells of g (eps(w + delta e_c) - eps(w - delta e_c)) / (2 delta), with
+ * eps from the fill rule at both ends of the step.  It differs from the
+ * derivative where the step moves an edge across a cell boundary (the fill is
+ * only piecewise linear in the width), and it is what a central difference of
+ * the simulated objective with step +-delta measures, to second order.  delta
+ * (um) may move an edge by at most one cell.  No reference counterpart. */
+int fdtd_spline_store_gradient_step(fdtd_spline_store store, double ep_diff, double delta, double *grad);
 void fdtd_spline_store_free(fdtd_spline_store store);
 
 /* BF16 GEMM on the tcgen05 tensor cores (no reference counterpart; the
@@ -451,6 +461,25 @@ void fdtd_inject_allocation_failures(int n);
  * limit_seconds (0 < limit <= 10), reported like a real pipeline timeout, with
  * the CUDA context still usable; *elapsed_seconds = the device-side wait. */
 int fdtd_wait_selftest(double limit_seconds, double *elapsed_seconds);
+/* Candidate sweep: advance `ngrids` grids together, grid i by nsteps[i] steps
+ * (uneven counts allowed), in persistent launches of up to steps_per_launch
+ * steps that run every grid's one-pass Yee update, monitors and scheduled
+ * source (captured as one CUDA graph on the library's sweep stream; returns
+ * at once, each grid's stream continues after it).  No reference counterpart:
+ * the reference runs one design at a time (3d_fdtd.c:93-202).  Each grid is
+ * set up as for timefield3d_run (FP32, CPML of the same thickness on all or
+ * PEC walls on all, the same loss, nx a multiple of 4, no probes or bound
+ * stores) and ends exactly as timefield3d_run would leave it.  Tile shape:
+ * band_rows caps the rows of a band (0: as many as shared memory allows);
+ * tiles_per_sm sets how many tiles per SM the grids are cut into per step
+ * (in (0, 16]).  A grid barrier that waits more than 1 s ends the launch;
+ * the grids then report FDTD_ERR_TIMEOUT at their next synchronising call. */
+int fdtd_sweep_run(const timefield3d *grids, int ngrids, double delta_t, const int *nsteps, int steps_per_launch,
+                   int band_rows, double tiles_per_sm);
+/* runs the sweep's grid barrier on a barrier nothing can complete, with a
+ * limit of limit_seconds (in (0, 10]); returns FDTD_ERR_TIMEOUT when the wait
+ * gave up as designed and the context stays usable.  No reference counterpart. */
+int fdtd_sweep_barrier_selftest(double limit_seconds);
 /* the grid's CUDA stream (cudaStream_t), for callers that order work or time it */
 void *timefield3d_get_stream(timefield3d psi);
 /* upload psi.ep/mu/sig now (otherwise done on the next device use after a change) */

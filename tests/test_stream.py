@@ -24,7 +24,7 @@ import pytest
 from make_golden import wg_geometry, wg_setup
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-SMEM_MAX = 232448
+SMEM_MAX = 231424
 
 
 def plan(fd, nx, ny, nz, L, lossy, nsm):
@@ -54,7 +54,15 @@ def test_stream_plan_covers_interior_once(fd, nx, ny, nz, L, lossy, nsm):
     assert p is not None
     tiles, ty, threads, smem = p
     assert 1 <= len(tiles) <= nsm
-    assert threads % 32 == 0 and (ty + 1) * (nx // 4) <= threads <= 384   # 12 warps x 168 registers fit an SM
+    # 12 warps x 168 registers fit an SM; x-slab quads (row ends) get warps of their own
+    qx = nx // 4
+    if L:
+        ql, qr = (L + 3) // 4, max((L + 3) // 4, min(qx, (nx - L) // 4))
+        qi = qr - ql
+        want = ((ty + 1) * qi + 31) // 32 * 32 + (ty + 1) * (qx - qi)
+    else:
+        want = (ty + 1) * qx
+    assert threads % 32 == 0 and threads == (want + 31) // 32 * 32 and threads <= 384
     na = 12 if lossy else 9
     xw = (2 * L + 3) // 4 * 4   # staged x-slab auxiliaries per row, padded to 16 bytes
     assert smem == ((3 * na * (ty + 1) + 6 + 6 * (ty + 1)) * nx + 3 * 4 * (ty + 1) * xw) * 4 <= SMEM_MAX

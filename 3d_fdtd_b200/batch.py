@@ -40,7 +40,6 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-MODES = os.path.join(ROOT, "tests", "golden", "modes")
 REF_PI = 3.141592652
 DP = C.POINTER(C.c_double)
 
@@ -75,6 +74,22 @@ def source_tables(T: int, dt: float):
     return np.exp(-((n - 3 * sigma_n) ** 2) / (2 * sigma_n ** 2)), n * dt * w0
 
 
+_MODES = {}
+
+
+def candidate_modes(fd):
+    """TE0 modes of the 0.5 um input and 3.0 um output strips on the candidates'
+    256 x 128 cross-section, from the library's GPU mode solver (once per process)."""
+    if "c" not in _MODES:
+        modes = importlib.import_module("3d_fdtd_b200.modes")
+        s = SPEC
+        b, top = s["core_y"]
+        _MODES["c"] = tuple(modes.strip_mode(fd, s["nx"], s["ny"], s["dx"], (x0, x1, b, top), s["ep_clad"],
+                                             s["ep_core"], s["lam0"], 20, 1e-8)[0]
+                            for x0, x1 in (s["w_in"], s["w_out"]))
+    return tuple(m.copy() for m in _MODES["c"])
+
+
 class Slot:
     """One resident simulation: a grid, its modes, monitors and source schedule."""
 
@@ -84,8 +99,7 @@ class Slot:
         self.shape = None
         self.cand = None
         self.variant = 0
-        self.mode_in = fd.read_mode_file(os.path.join(MODES, "c1_in_te0.txt.gz"))
-        self.mode_out = fd.read_mode_file(os.path.join(MODES, "c1_out_te0.txt.gz"))
+        self.mode_in, self.mode_out = candidate_modes(fd)
         self.omega = np.array([2 * REF_PI / l for l in SPEC["lams"]])
 
     def prepare(self, cand: dict, variant: int = 0, retire: list | None = None) -> None:
@@ -231,12 +245,95 @@ def sweep(fd, cands: list[dict], slots: int = 4, variant: int | None = None, ret
                 variant=variant, tuning={int(k): v for k, v in tuning.items()})
 
 
+def _sweep_call(fd, slots, nsteps, steps_per_launch, band_rows, tiles_per_sm):
+    grids = (fd.Timefield3d * len(slots))(*[s.grid.t for s in slots])
+    n = (C.c_int * len(slots))(*nsteps)
+    fd.call("fdtd_sweep_run", grids, len(slots), slots[0].dt, n, steps_per_launch, band_rows, tiles_per_sm)
+
+
+def autotune_tiles(fd, cands: list[dict], steps: int = 128, steps_per_launch: int = 64,
+                   shapes=((0, 1.0), (0, 2.0), (4, 1.0), (3, 1.0), (3, 2.0))) -> tuple[tuple[int, float], dict]:
+    """Tile shape of the persistent sweep: for each (band rows cap, tiles per
+    SM) the sweep of these candidates runs `steps` steps after a warm-up, timed
+    on the host around a synchronised call; the fastest shape is returned."""
+    slots = []
+    for c in cands:
+        s = Slot(fd)
+        s.prepare(dict(c, steps=max(c["steps"], steps)), fd.YEE_STREAM)
+        slots.append(s)
+    times = {}
+    for shape in shapes:
+        for s in slots:
+            fd.lib.timefield3d_zero_fields(s.grid.t)
+        _sweep_call(fd, slots, [steps_per_launch] * len(slots), steps_per_launch, *shape)   # warm-up (graph, plan)
+        for s in slots:
+            fd.call("timefield3d_synchronize", s.grid.t)
+        t0 = time.perf_counter()
+        _sweep_call(fd, slots, [steps] * len(slots), steps_per_launch, *shape)
+        for s in slots:
+            fd.call("timefield3d_synchronize", s.grid.t)
+        times[shape] = (time.perf_counter() - t0) / steps * 1e3
+    for s in slots:
+        s.close()
+    best = min(times, key=times.get)
+    return best, times
+
+
+def sweep_persistent(fd, cands: list[dict], group: int = 8, steps_per_launch: int = 64,
+                     shape: tuple[int, float] | None = None) -> dict:
+    """Every candidate through persistent sweep launches: candidates sorted by
+    step count, `group` at a time advance together (uneven lengths inside the
+    launches); the next group is set up on the host while the current one runs."""
+    if not cands:
+        return dict(results={}, amplitudes={}, seconds=0.0, cell_steps=0, bytes=0, shape=None, tuning={})
+    order = sorted(cands, key=lambda c: c["steps"])
+    groups = [order[i:i + group] for i in range(0, len(order), group)]
+    tuning = {}
+    if shape is None:
+        shape, tuning = autotune_tiles(fd, groups[-1][:group])
+    results, amplitudes = {}, {}
+    cell_steps = nbytes = 0
+    t0 = time.perf_counter()
+    current = []
+    for c in groups[0]:
+        s = Slot(fd)
+        s.prepare(c, fd.YEE_STREAM)
+        fd.lib.timefield3d_zero_fields(s.grid.t)
+        current.append(s)
+    for gi in range(len(groups)):
+        _sweep_call(fd, current, [s.cand["steps"] for s in current], steps_per_launch, *shape)
+        nxt = []
+        if gi + 1 < len(groups):
+            for c in groups[gi + 1]:
+                s = Slot(fd)
+                s.prepare(c, fd.YEE_STREAM)
+                fd.lib.timefield3d_zero_fields(s.grid.t)
+                nxt.append(s)
+        for s in current:
+            c = s.cand
+            t = s.amplitudes()
+            amplitudes[c["index"]] = t
+            results[c["index"]] = (np.abs(t) ** 2).tolist()
+            nx, ny, nz = s.shape
+            cell_steps += nx * ny * nz * c["steps"]
+            nbytes += algorithmic_bytes(nx, ny, nz, SPEC["cpml"]) * c["steps"]
+        for s in current:
+            s.close()
+        current = nxt
+    seconds = time.perf_counter() - t0
+    return dict(results=results, amplitudes=amplitudes, seconds=seconds, cell_steps=cell_steps, bytes=nbytes,
+                shape=list(shape), tuning={f"{k[0]}x{k[1]}": v for k, v in tuning.items()})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--candidates", type=int, default=64)
     ap.add_argument("--slots", type=int, default=4)
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--steps-scale", type=float, default=1.0)
+    ap.add_argument("--mode", choices=["persistent", "slots"], default="persistent",
+                    help="persistent: groups of candidates in persistent sweep launches; slots: one run per slot")
+    ap.add_argument("--group", type=int, default=8)
     args = ap.parse_args()
     import torch
 
@@ -249,7 +346,11 @@ def main():
     cands = candidates(args.candidates, args.seed, steps_scale=args.steps_scale)
     mine = [cands[i] for i in ranks.shard(len(cands))]
     ranks.barrier()
-    r = sweep(fd, mine, args.slots)
+    if args.mode == "persistent":
+        r = sweep_persistent(fd, mine, args.group)
+        r["variant"] = "persistent sweep"
+    else:
+        r = sweep(fd, mine, args.slots)
     seconds = ranks.max(r["seconds"])
     per_rank = ranks.gather(dict(cell_steps=r["cell_steps"], bytes=r["bytes"]))
     T = ranks.gather_shards(len(cands), r["results"])
@@ -261,6 +362,7 @@ def main():
         line = dict(metric="candidate sweep Yee Mcell-updates/s", value=cell_steps / seconds / 1e6,
                     unit="Mcell-updates/s", n_gpus=ranks.world, candidates=len(cands), seconds=seconds,
                     hbm_frac=nbytes / seconds / 1e9 / (peak * ranks.world), slots=args.slots,
+                    mode=args.mode, group=args.group, tile_shape=r.get("shape"),
                     variant=r["variant"], tuning_ms_per_step=r["tuning"],
                     T_mean_1550=float(np.mean([t[5] for t in T])),
                     T_best_1550=float(np.max([t[5] for t in T])))

@@ -88,18 +88,32 @@ __device__ __forceinline__ void stream_yzpsi_load(YZPsi &s, const StreamArgs &a,
     }
 }
 
+// a quad wholly inside one x slab, with its auxiliaries 16-byte aligned (L
+// even): moved as one vector; the elements x = 0 / nx-1 hold 0, which is their
+// auxiliaries' value for good (they are never updated)
+__device__ __forceinline__ bool xquad_whole(int i0, int nx, int L)
+{
+    return (L & 1) == 0 && (i0 + 3 < L || i0 >= nx - L);
+}
+
 template <int A0>
 __device__ __forceinline__ void stream_psi_store(const XPsi &xs, const YZPsi &s, const StreamArgs &a, int q, int j,
-                                                 int k, long long ij0, long long nxy)
+                                                 int k, long long ij0, long long nxy, bool xquad)
 {
     const int nx = a.nx, L = a.L, i0 = 4 * q;
     const long long s0 = 2LL * L * (j + (long long)a.ny * k);
+    if (xquad && xquad_whole(i0, nx, L)) {
+        const long long si = s0 + slab_local(i0, nx, L);
+        *reinterpret_cast<float4 *>(a.psi_out[0][A0] + si) = make_float4(xs.p0[0], xs.p0[1], xs.p0[2], xs.p0[3]);
+        *reinterpret_cast<float4 *>(a.psi_out[0][A0 + 1] + si) = make_float4(xs.p1[0], xs.p1[1], xs.p1[2], xs.p1[3]);
+    } else if (xquad) {
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-        if (!xs.valid[e]) continue;
-        const long long sidx = s0 + slab_local(i0 + e, nx, L);
-        a.psi_out[0][A0][sidx] = xs.p0[e];
-        a.psi_out[0][A0 + 1][sidx] = xs.p1[e];
+        for (int e = 0; e < 4; e++) {
+            if (!xs.valid[e]) continue;
+            const long long sidx = s0 + slab_local(i0 + e, nx, L);
+            a.psi_out[0][A0][sidx] = xs.p0[e];
+            a.psi_out[0][A0 + 1][sidx] = xs.p1[e];
+        }
     }
     if (s.sj >= 0) {
         const long long sy = (long long)i0 + (long long)nx * (s.sj + 2LL * L * k);
@@ -353,12 +367,20 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
             }
             if (CPML && xw && !h_only) {
                 const long long xs0 = 2LL * L * (j + (long long)ny * k);
+                const int si0 = slab_local(i0, nx, L);
+                if (xquad_whole(i0, nx, L)) {
+                    // the quad lies in one slab and its 4 auxiliaries are 16-byte aligned
 #pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const int si = slab_local(i0 + e, nx, L);
-                    if (si < 0) continue;
+                    for (int arr = 0; arr < 4; arr++) cp_async16(xrow(s, arr, r) + si0, a.psi_in[0][arr] + xs0 + si0);
+                } else {
 #pragma unroll
-                    for (int arr = 0; arr < 4; arr++) cp_async4(xrow(s, arr, r) + si, a.psi_in[0][arr] + xs0 + si);
+                    for (int e = 0; e < 4; e++) {
+                        const int si = slab_local(i0 + e, nx, L);
+                        if (si < 0) continue;
+#pragma unroll
+                        for (int arr = 0; arr < 4; arr++)
+                            cp_async4(xrow(s, arr, r) + si, a.psi_in[0][arr] + xs0 + si);
+                    }
                 }
             }
         }
@@ -369,18 +391,23 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
     issue(1, false);
     const float dx = a.dx, div = 1.0f / dx, hb = a.hb;
     const bool row_upd = j >= 1 && j <= ny - 2;      // false only for a halo row on the shell
+    // y- and z-slab auxiliaries of iteration `it`'s updates (E of plane k, H of
+    // plane k-1), read from global memory one iteration ahead
+    YZPsi yze, yzh;
+    auto load_yz = [&](int it) {
+        yze.sj = yze.sk = yzh.sj = yzh.sk = -1;
+        if (!CPML || it > n) return;
+        const int k = tl.k0 + it;
+        if (act && row_upd && k <= nz - 2) stream_yzpsi_load<0, COH>(yze, a, q, j, k, ij0, nxy);
+        if (own && it >= 1) stream_yzpsi_load<2, COH>(yzh, a, q, j, k - 1, ij0, nxy);
+    };
+    load_yz(0);
 
     for (int it = 0; it <= n; it++) {
         const int k = tl.k0 + it;
         const int s = it % S, sp_ = (it + S - 1) % S;      // this plane's stage, the previous plane's
         const bool e_upd = act && row_upd && k <= nz - 2;   // k >= 1 always
         const bool h_upd = own && it >= 1;
-        // y- and z-slab auxiliaries of both updates, loaded before the wait so
-        // their latency overlaps it
-        YZPsi yze, yzh;
-        yze.sj = yze.sk = yzh.sj = yzh.sk = -1;
-        if (CPML && e_upd) stream_yzpsi_load<0, COH>(yze, a, q, j, k, ij0, nxy);
-        if (CPML && h_upd) stream_yzpsi_load<2, COH>(yzh, a, q, j, k - 1, ij0, nxy);
         cp_async_wait_group<1>();   // this thread's copies up to iteration it have landed
         __syncthreads();            // ... and everyone's; new E of iteration it-1 visible
         // own slots of the previous plane's stage: old H (the E update's z
@@ -444,10 +471,7 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
             stv<4>(a.f_out[0] + g, ex);
             stv<4>(a.f_out[1] + g, ey);
             stv<4>(a.f_out[2] + g, ez);
-            if (CPML) {
-                if (!xw) xse.valid[0] = xse.valid[1] = xse.valid[2] = xse.valid[3] = false;
-                stream_psi_store<0>(xse, yze, a, q, j, k, ij0, nxy);
-            }
+            if (CPML) stream_psi_store<0>(xse, yze, a, q, j, k, ij0, nxy, xw);
         }
 
         // ---- H_new(k-1) of rows j0..j0+R-1: own old H and x-slab auxiliaries
@@ -476,11 +500,9 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
             stv<4>(a.f_out[3] + g, nhx);
             stv<4>(a.f_out[4] + g, nhy);
             stv<4>(a.f_out[5] + g, nhz);
-            if (CPML) {
-                if (!xw) xsh.valid[0] = xsh.valid[1] = xsh.valid[2] = xsh.valid[3] = false;
-                stream_psi_store<2>(xsh, yzh, a, q, j, km, ij0, nxy);
-            }
+            if (CPML) stream_psi_store<2>(xsh, yzh, a, q, j, km, ij0, nxy, xw);
         }
+        load_yz(it + 1);
     }
     cp_async_wait_group<0>();
 }

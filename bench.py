@@ -36,7 +36,9 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
-MODES = os.path.join(ROOT, "tests", "golden", "modes")
+# modes written by the reference's own solver (test fixtures): used only by the
+# reference's CPU arm, which loads modes through its own mode_file_load
+REF_MODES = os.path.join(ROOT, "tests", "golden", "modes")
 REF_PI = 3.141592652
 
 # ---------------------------------------------------------------------------
@@ -83,6 +85,25 @@ def rasterise(lib, t):
 
 def dptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+_MODES = {}
+
+
+def taper_modes(fd):
+    """TE0 modes of the taper's input (0.5 um) and output (3.0 um) strips on the
+    full 200 x 160 cross-section, from the library's GPU mode solver (solved once
+    per process, outside every timed region)."""
+    if "taper" not in _MODES:
+        modes = importlib.import_module("3d_fdtd_b200.modes")
+        b, top = W["core_y"]
+        out = []
+        for x0, x1 in (W["w_in"], W["w_out"]):
+            m, _ = modes.strip_mode(fd, W["nx"], W["ny"], W["dx"], (x0, x1, b, top), W["ep_clad"], W["ep_core"],
+                                    W["lam0"], 20, 1e-8)
+            out.append(m)
+        _MODES["taper"] = tuple(out)
+    return tuple(m.copy() for m in _MODES["taper"])
 
 
 # ---------------------------------------------------------------------------
@@ -156,7 +177,7 @@ class ReferenceRun:
         self.modes = []
         for name in ("c1_in_te0", "c1_out_te0"):
             txt = os.path.join(tmp, name + ".txt")
-            with gzip.open(os.path.join(MODES, name + ".txt.gz"), "rb") as fi, open(txt, "wb") as fo:
+            with gzip.open(os.path.join(REF_MODES, name + ".txt.gz"), "rb") as fi, open(txt, "wb") as fo:
                 shutil.copyfileobj(fi, fo)
             self.modes.append(R.load_mode(txt))
         shutil.rmtree(tmp)
@@ -247,8 +268,7 @@ class Taper:
         else:   # analysis only: the same grid with PEC walls (no CPML terms)
             fd.call("timefield3d_set_boundary", self.t, fd.PEC)
         fd.call("timefield3d_set_yee_variant", self.t, variant)
-        self.mode_in = fd.read_mode_file(os.path.join(MODES, "c1_in_te0.txt.gz"))
-        self.mode_out = fd.read_mode_file(os.path.join(MODES, "c1_out_te0.txt.gz"))
+        self.mode_in, self.mode_out = taper_modes(fd)
         self.amp, self.phase = source_tables(time_steps, self.dt)
         self.omega = np.array([2 * REF_PI / l for l in W["lams"]])
         fd.call("timefield3d_upload_materials", self.t)
@@ -384,6 +404,19 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = world * cells * args.time_steps * args.steps / e2e_s / 1e6
+    # candidate sweep (64-candidate taper family, seeded subset): persistent
+    # multi-grid launches with the tile-shape autotuner, host clock around it
+    sweep = None
+    if rank == 0 and world == 1 and args.sweep_candidates > 0:
+        batch = importlib.import_module("3d_fdtd_b200.batch")
+        cands = batch.candidates(64, seed=2)[:args.sweep_candidates]
+        r = batch.sweep_persistent(fd, cands, group=len(cands))
+        peak_gbs, _ = peaks()
+        sweep = {"candidates": len(cands), "of": "64-candidate taper family (seed 2), first candidates",
+                 "value": r["cell_steps"] / r["seconds"] / 1e6, "unit": "Mcell-updates/s",
+                 "hbm_frac": r["bytes"] / r["seconds"] / 1e9 / peak_gbs, "seconds": r["seconds"],
+                 "tile_shape": r["shape"], "autotune_ms_per_step": r["tuning"],
+                 "launch": "persistent cooperative launches of 64 steps over all candidates, one CUDA graph"}
     # FP32 against FP64: the same workload once on the engine's FP64 path (bit-exact
     # to the CPU restatement on CPML grids), outside every timed region
     t32 = sim.amplitude_ratio()
@@ -411,7 +444,7 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
         line = {"metric": "Yee Mcell-updates/s", "value": value, "unit": "Mcell-updates/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (seeded geometry and mode profiles generated by the reference's mode solver)",
+                "data": "synthetic (seeded geometry; TE0 modes from the library's GPU mode solver on the 200x160 cross-section)",
                 "config": config_block(args),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
@@ -424,7 +457,7 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e, "unit": "Mcell-updates/s", "h2d_bytes_per_step": sim.h2d_bytes(),
                         "d2h_bytes_per_step": sim.d2h_bytes()},
-                "gpu_launches": launches, "clocks": clk,
+                "gpu_launches": launches, "clocks": clk, "sweep": sweep,
                 "transmission": {"lambda_um": W["lams"], "T": [round(float(x), 6) for x in trans],
                                  "T_e2e_equal": bool(np.allclose(trans, trans_e2e, rtol=1e-6)),
                                  **(f64_check or {})}}
@@ -442,6 +475,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-f64-check", action="store_true", help="skip the FP64 run that checks the FP32 transmission")
+    ap.add_argument("--sweep-candidates", type=int, default=8,
+                    help="candidates of the taper family in the sweep measurement (0: skip)")
     ap.add_argument("--boundary", choices=["cpml", "pec"], default="cpml",
                     help="pec: analysis of the update without CPML terms (not the bench workload)")
     ap.add_argument("--yee-variant", choices=["auto", "flat", "flat4", "fused", "wave", "stream"], default="auto")

@@ -55,3 +55,30 @@ def test_autotune_times_each_design(fd, gpu, B):
     best, times = B.autotune(fd, c, steps=32)
     assert set(times) == {fd.YEE_FLAT4, fd.YEE_FLAT, fd.YEE_FUSED}
     assert best == min(times, key=times.get) and all(v > 0 for v in times.values())
+
+
+@pytest.mark.gpu
+def test_persistent_sweep_equals_single_runs(fd, gpu, B):
+    # three candidates of different lengths advance together in persistent
+    # launches; each equals the same candidate run alone on the one-pass kernel
+    cands = B.candidates(3, seed=2)
+    r = B.sweep_persistent(fd, cands, group=3, shape=(0, 1.0))
+    assert sorted(r["results"]) == [0, 1, 2]
+    for c in cands:
+        s = B.Slot(fd)
+        s.prepare(c, fd.YEE_STREAM)
+        s.start()
+        alone = s.amplitudes()
+        s.close()
+        got = r["amplitudes"][c["index"]]
+        assert np.all(np.isfinite(got)) and 0.05 < np.abs(got).max() ** 2 < 1.5
+        assert np.array_equal(got, alone)
+    assert r["cell_steps"] == sum(256 * 128 * c["nz"] * c["steps"] for c in cands)
+
+
+@pytest.mark.gpu
+def test_tile_autotuner_times_each_shape(fd, gpu, B):
+    cands = B.candidates(2, seed=2)
+    shapes = ((0, 1.0), (3, 2.0))
+    best, times = B.autotune_tiles(fd, cands, steps=64, shapes=shapes)
+    assert set(times) == set(shapes) and best == min(times, key=times.get) and all(v > 0 for v in times.values())

@@ -241,7 +241,8 @@ def reference_arm(args, rank: int) -> None:
 
 def config_block(args) -> dict:
     return {"workload": WORKLOAD_NAME, "grid": [W["nx"], W["ny"], W["nz"]], "dx_um": W["dx"],
-            "time_steps": args.time_steps, "cpml_cells": W["cpml"] if getattr(args, "boundary", "cpml") == "cpml" else 0,
+            "time_steps": args.time_steps,
+            "cpml_cells": (getattr(args, "cpml_cells", None) or W["cpml"]) if getattr(args, "boundary", "cpml") == "cpml" else 0,
             "n_lambda": len(W["lams"]),
             "lambda_um": [W["lams"][0], W["lams"][-1]], "fields": "f32", "monitors": "f64 compensated",
             "taper_um": [0.5, 3.0], "taper_length_um": (W["taper_z"][1] - W["taper_z"][0]) * W["dx"],
@@ -255,7 +256,8 @@ def config_block(args) -> dict:
 class Taper:
     """One simulation of the workload on one GPU."""
 
-    def __init__(self, fd, time_steps: int, variant: int = 0, precision: int | None = None, boundary: str = "cpml"):
+    def __init__(self, fd, time_steps: int, variant: int = 0, precision: int | None = None, boundary: str = "cpml",
+                 cpml_cells: int | None = None):
         self.fd, self.T = fd, time_steps
         lib = fd.lib
         nx, ny, nz, dx = W["nx"], W["ny"], W["nz"], W["dx"]
@@ -263,8 +265,9 @@ class Taper:
         self.grid = fd.Grid(nx, ny, nz, dx, fd.F32 if precision is None else precision)
         self.t = self.grid.t
         rasterise(lib, self.t)
+        self.L = W["cpml"] if cpml_cells is None else cpml_cells
         if boundary == "cpml":
-            fd.call("timefield3d_set_cpml", self.t, W["cpml"], 3, -1.0, 1.0, 0.0)
+            fd.call("timefield3d_set_cpml", self.t, self.L, 3, -1.0, 1.0, 0.0)
         else:   # analysis only: the same grid with PEC walls (no CPML terms)
             fd.call("timefield3d_set_boundary", self.t, fd.PEC)
         fd.call("timefield3d_set_yee_variant", self.t, variant)
@@ -351,7 +354,7 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
     barrier, max_over_ranks = ranks.barrier, ranks.max
 
     sim = Taper(fd, args.time_steps, {"auto": 0, "flat": 1, "fused": 2, "flat4": 3, "wave": 4, "stream": 5}[args.yee_variant],
-                boundary=args.boundary)
+                boundary=args.boundary, cpml_cells=args.cpml_cells)
     stream = torch.cuda.ExternalStream(fd.lib.timefield3d_get_stream(sim.t))
     cells = W["nx"] * W["ny"] * W["nz"]
     # warm-up: full runs (graph capture, clocks)
@@ -388,7 +391,7 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
     trans = sim.transmission()
     # roofline of the Yee update (E + H kernels with CPML), measured inside the timed runs
     kms = ktot.value / max(kcnt.value, 1)
-    bytes_step = algorithmic_bytes_per_step(W["nx"], W["ny"], W["nz"], W["cpml"] if args.boundary == "cpml" else 0)
+    bytes_step = algorithmic_bytes_per_step(W["nx"], W["ny"], W["nz"], sim.L if args.boundary == "cpml" else 0)
     achieved = bytes_step / (kms / 1e3) / 1e9
     peak, peak_kind = peaks()
     wave = args.yee_variant == "wave"
@@ -477,6 +480,8 @@ def main():
     ap.add_argument("--no-f64-check", action="store_true", help="skip the FP64 run that checks the FP32 transmission")
     ap.add_argument("--sweep-candidates", type=int, default=8,
                     help="candidates of the taper family in the sweep measurement (0: skip)")
+    ap.add_argument("--cpml-cells", type=int, default=None,
+                    help="analysis only: CPML thickness other than the workload's 12 cells")
     ap.add_argument("--boundary", choices=["cpml", "pec"], default="cpml",
                     help="pec: analysis of the update without CPML terms (not the bench workload)")
     ap.add_argument("--yee-variant", choices=["auto", "flat", "flat4", "fused", "wave", "stream"], default="auto")

@@ -39,8 +39,10 @@ __device__ __forceinline__ void sts4(float *p, const Vf<4> &x)
 // ---- CPML auxiliaries of one quad for one field (E: A0 = 0, H: A0 = 2).
 //      x-slab: per element, staged in shared memory with the plane (rows of
 //      2L values); y- and z-slab: contiguous in x, read from global memory.
-//      The 1-D profiles are read where they are used (a few hundred floats,
-//      cached).
+//      The 1-D profiles of the slab cells sit in a shared table filled at the
+//      start of the tile (stream_profile_table): read from global memory at
+//      every use they missed L1 (the staged planes leave it a few KB) and put
+//      an L2 round trip on every x-slab cell's update.
 struct XPsi {
     bool valid[4];
     float p0[4], p1[4];
@@ -63,6 +65,24 @@ __device__ __forceinline__ void stream_xpsi(XPsi &xs, const float *row0, const f
         xs.valid[e] = any && si >= 0 && i >= 1 && i <= nx - 2;
         xs.p0[e] = xs.valid[e] ? row0[si] : 0.f;
         xs.p1[e] = xs.valid[e] ? row1[si] : 0.f;
+    }
+}
+
+// Shared profile table of a tile: [axis x, y, z][profile 0..5][2L slab-local
+// cells] (profiles 0..2: b, a, 1/kappa of E; 3..5 of H; slab-local index as
+// slab_local), filled by the whole block.  The caller's first barrier orders
+// the fill before any read.
+__device__ __forceinline__ void stream_profile_table(float *pt, const StreamArgs &a)
+{
+    const int L = a.L, PL = 2 * L;
+    for (int s = (int)threadIdx.x; s < PL; s += (int)blockDim.x) {
+#pragma unroll
+        for (int ax = 0; ax < 3; ax++) {
+            const int N = ax == 0 ? a.nx : (ax == 1 ? a.ny : a.nz);
+            const int g = s < L ? s : N - PL + s;
+#pragma unroll
+            for (int w = 0; w < 6; w++) pt[(ax * 6 + w) * PL + s] = __ldg(a.prof[w][ax] + g);
+        }
     }
 }
 
@@ -128,19 +148,22 @@ __device__ __forceinline__ void stream_psi_store(const XPsi &xs, const YZPsi &s,
 }
 
 // One cell's curl with the CPML terms: the arithmetic of cpml_curl
-// (flat4_cells.cuh) term for term, with the profiles read here.  pw = 0 for E
-// (b, a, 1/kappa of E), 3 for H.  X: the cell may lie in an x slab (its x
-// terms are compiled in); without X the x terms are the interior's (kappa 1,
-// no auxiliary), exactly what the general expression gives there.
+// (flat4_cells.cuh) term for term, with the profiles from the tile's shared
+// table `pt` (stream_profile_table).  pw = 0 for E (b, a, 1/kappa of E), 3 for
+// H.  X: the cell may lie in an x slab (its x terms are compiled in); without
+// X the x terms are the interior's (kappa 1, no auxiliary), exactly what the
+// general expression gives there.
 template <bool X, int pw>
-__device__ __forceinline__ Curl3 stream_cpml_curl(XPsi &xs, YZPsi &s, const StreamArgs &a, int i, int j, int k, int e,
+__device__ __forceinline__ Curl3 stream_cpml_curl(XPsi &xs, YZPsi &s, const float *pt, int nx, int L, int i, int e,
                                                   float d_zy, float d_yz, float d_xz, float d_zx, float d_yx,
                                                   float d_xy, float dx, float div)
 {
+    const int PL = 2 * L;
     float pyx = 0.f, pzx = 0.f, kx = 1.f;
     if (X && xs.valid[e]) {
-        const float b = __ldg(a.prof[pw + 0][0] + i), c = __ldg(a.prof[pw + 1][0] + i);
-        kx = __ldg(a.prof[pw + 2][0] + i);
+        const float *px = pt + pw * PL + slab_local(i, nx, L);
+        const float b = px[0], c = px[PL];
+        kx = px[2 * PL];
         pyx = b * xs.p0[e] + c * (d_zx * div);
         pzx = b * xs.p1[e] + c * (d_yx * div);
         xs.p0[e] = pyx;
@@ -148,16 +171,18 @@ __device__ __forceinline__ Curl3 stream_cpml_curl(XPsi &xs, YZPsi &s, const Stre
     }
     float vxy = 0.f, vzy = 0.f, vxz = 0.f, vyz = 0.f, ky = 1.f, kz = 1.f;
     if (s.sj >= 0) {
-        const float by = __ldg(a.prof[pw + 0][1] + j), ay = __ldg(a.prof[pw + 1][1] + j);
-        ky = __ldg(a.prof[pw + 2][1] + j);
+        const float *py = pt + (6 + pw) * PL + s.sj;
+        const float by = py[0], ay = py[PL];
+        ky = py[2 * PL];
         vxy = by * s.pxy.v[e] + ay * (d_zy * div);
         vzy = by * s.pzy.v[e] + ay * (d_xy * div);
         s.pxy.v[e] = vxy;
         s.pzy.v[e] = vzy;
     }
     if (s.sk >= 0) {
-        const float bz = __ldg(a.prof[pw + 0][2] + k), az = __ldg(a.prof[pw + 1][2] + k);
-        kz = __ldg(a.prof[pw + 2][2] + k);
+        const float *pz = pt + (12 + pw) * PL + s.sk;
+        const float bz = pz[0], az = pz[PL];
+        kz = pz[2 * PL];
         vxz = bz * s.pxz.v[e] + az * (d_yz * div);
         vyz = bz * s.pyz.v[e] + az * (d_xz * div);
         s.pxz.v[e] = vxz;
@@ -219,7 +244,7 @@ __device__ __forceinline__ void stream_e_quad(Vf<4> &ex, Vf<4> &ey, Vf<4> &ez, c
                                               const Vf<4> &hx_jm, const Vf<4> &hz_jm, float hy_im0, float hz_im0,
                                               const Vf<4> &b0, const Vf<4> &b1, const Vf<4> &b2, const Vf<4> &c0,
                                               const Vf<4> &c1, const Vf<4> &c2, XPsi &xs, YZPsi &yz,
-                                              const StreamArgs &a, int i0, int j, int k, const float *sp,
+                                              const float *pt, const StreamArgs &a, int i0, const float *sp,
                                               long long ij0, long long nxy, float dx, float div)
 {
     const bool plain = !CPML || (!X && yz.sj < 0 && yz.sk < 0);
@@ -241,8 +266,8 @@ __device__ __forceinline__ void stream_e_quad(Vf<4> &ex, Vf<4> &ey, Vf<4> &ez, c
             cy = dHx_dz - dHz_dx;
             cz = dHy_dx - dHx_dy;
         } else {
-            const Curl3 c = stream_cpml_curl<X, 0>(xs, yz, a, i, j, k, e, dHz_dy, dHy_dz, dHx_dz, dHz_dx, dHy_dx,
-                                                   dHx_dy, dx, div);
+            const Curl3 c = stream_cpml_curl<X, 0>(xs, yz, pt, a.nx, a.L, i, e, dHz_dy, dHy_dz, dHx_dz, dHz_dx,
+                                                   dHy_dx, dHx_dy, dx, div);
             cx = c.x; cy = c.y; cz = c.z;
         }
         if (sp) {
@@ -261,7 +286,7 @@ template <bool X, bool EDGE, bool CPML, bool COH>
 __device__ __forceinline__ void stream_h_quad(Vf<4> &nhx, Vf<4> &nhy, Vf<4> &nhz, const Vf<4> &ex, const Vf<4> &ey,
                                               const Vf<4> &exm, const Vf<4> &eym, const Vf<4> &ezm,
                                               const Vf<4> &ex_jp, const Vf<4> &ez_jp, float ey_ipw, float ez_ipw,
-                                              XPsi &xs, YZPsi &yz, const StreamArgs &a, int i0, int j, int km,
+                                              XPsi &xs, YZPsi &yz, const float *pt, const StreamArgs &a, int i0,
                                               const float *sp, long long ij0, long long nxy, float dx, float div,
                                               float hb)
 {
@@ -284,8 +309,8 @@ __device__ __forceinline__ void stream_h_quad(Vf<4> &nhx, Vf<4> &nhy, Vf<4> &nhz
             cy = dEx_dz - dEz_dx;
             cz = dEy_dx - dEx_dy;
         } else {
-            const Curl3 c = stream_cpml_curl<X, 3>(xs, yz, a, i, j, km, e, dEz_dy, dEy_dz, dEx_dz, dEz_dx, dEy_dx,
-                                                   dEx_dy, dx, div);
+            const Curl3 c = stream_cpml_curl<X, 3>(xs, yz, pt, a.nx, a.L, i, e, dEz_dy, dEy_dz, dEx_dz, dEz_dx,
+                                                   dEy_dx, dEx_dy, dx, div);
             cx = c.x; cy = c.y; cz = c.z;
         }
         if (sp) {
@@ -336,6 +361,8 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
     float *xps = stage + (size_t)S * NA * TP * nx;   // [S][4][TP][XW]: x-slab auxiliaries E0 E1 H0 H1
     float *hlow = xps + (size_t)S * 4 * TP * XW;     // [S][2][nx]: Hx, Hz of row j0-1
     float *es = hlow + (size_t)S * 2 * nx;           // [2][3][TP][nx]: new E of the last two planes
+    float *ptab = es + (size_t)2 * 3 * TP * nx;      // CPML profiles of the slab cells (stream_profile_table)
+    if (CPML) stream_profile_table(ptab, a);
     auto stg = [&](int s, int arr, int row) -> float * { return stage + ((size_t)(s * NA + arr) * TP + row) * nx; };
     auto xrow = [&](int s, int arr, int row) -> float * { return xps + ((size_t)(s * 4 + arr) * TP + row) * XW; };
     auto esp = [&](int b, int c, int row) -> float * { return es + ((size_t)(b * 3 + c) * TP + row) * nx; };
@@ -394,10 +421,17 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
     // y- and z-slab auxiliaries of iteration `it`'s updates (E of plane k, H of
     // plane k-1), read from global memory one iteration ahead
     YZPsi yze, yzh;
+    // Iterations whose planes hold no y- or z-slab cell of the tile's rows
+    // (block-uniform): interior quads run the plain updates there, with no
+    // auxiliary state; the general CPML expression computes the same values
+    // there (kappa 1, no auxiliaries).
+    const bool y_rows = CPML && (tl.j0 < L || tl.j0 + R >= ny - L);
+    auto yz_plane = [&](int k) { return y_rows || (CPML && (k < L || k >= nz - L)); };
     auto load_yz = [&](int it) {
         yze.sj = yze.sk = yzh.sj = yzh.sk = -1;
         if (!CPML || it > n) return;
         const int k = tl.k0 + it;
+        if (!xw && !yz_plane(k) && !yz_plane(k - 1)) return;
         if (act && row_upd && k <= nz - 2) stream_yzpsi_load<0, COH>(yze, a, q, j, k, ij0, nxy);
         if (own && it >= 1) stream_yzpsi_load<2, COH>(yzh, a, q, j, k - 1, ij0, nxy);
     };
@@ -449,15 +483,19 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
             const float *sp = a.src.n ? src_plane(a.src, k) : nullptr;
             if (!CPML)
                 stream_e_quad<false, true, false, LOSSY, COH>(ex, ey, ez, hx, hy, hz, hxm, hym, hx_jm, hz_jm, hy_im0,
-                                                              hz_im0, b0, b1, b2, c0, c1, c2, xse, yze, a, i0, j, k,
+                                                              hz_im0, b0, b1, b2, c0, c1, c2, xse, yze, ptab, a, i0,
                                                               sp, ij0, nxy, dx, div);
             else if (xw)
                 stream_e_quad<true, true, true, LOSSY, COH>(ex, ey, ez, hx, hy, hz, hxm, hym, hx_jm, hz_jm, hy_im0,
-                                                            hz_im0, b0, b1, b2, c0, c1, c2, xse, yze, a, i0, j, k, sp,
+                                                            hz_im0, b0, b1, b2, c0, c1, c2, xse, yze, ptab, a, i0, sp,
                                                             ij0, nxy, dx, div);
+            else if (!yz_plane(k))
+                stream_e_quad<false, false, false, LOSSY, COH>(ex, ey, ez, hx, hy, hz, hxm, hym, hx_jm, hz_jm, hy_im0,
+                                                               hz_im0, b0, b1, b2, c0, c1, c2, xse, yze, ptab, a, i0,
+                                                               sp, ij0, nxy, dx, div);
             else
                 stream_e_quad<false, false, true, LOSSY, COH>(ex, ey, ez, hx, hy, hz, hxm, hym, hx_jm, hz_jm, hy_im0,
-                                                              hz_im0, b0, b1, b2, c0, c1, c2, xse, yze, a, i0, j, k,
+                                                              hz_im0, b0, b1, b2, c0, c1, c2, xse, yze, ptab, a, i0,
                                                               sp, ij0, nxy, dx, div);
         }
         if (act) {
@@ -471,7 +509,7 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
             stv<4>(a.f_out[0] + g, ex);
             stv<4>(a.f_out[1] + g, ey);
             stv<4>(a.f_out[2] + g, ez);
-            if (CPML) stream_psi_store<0>(xse, yze, a, q, j, k, ij0, nxy, xw);
+            if (CPML && (xw || yz_plane(k))) stream_psi_store<0>(xse, yze, a, q, j, k, ij0, nxy, xw);
         }
 
         // ---- H_new(k-1) of rows j0..j0+R-1: own old H and x-slab auxiliaries
@@ -489,18 +527,21 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
             const float *sp = a.src.n ? src_plane(a.src, km) : nullptr;
             if (!CPML)
                 stream_h_quad<false, true, false, COH>(nhx, nhy, nhz, ex, ey, exm, eym, ezm, ex_jp, ez_jp, ey_ipw,
-                                                       ez_ipw, xsh, yzh, a, i0, j, km, sp, ij0, nxy, dx, div, hb);
+                                                       ez_ipw, xsh, yzh, ptab, a, i0, sp, ij0, nxy, dx, div, hb);
             else if (xw)
                 stream_h_quad<true, true, true, COH>(nhx, nhy, nhz, ex, ey, exm, eym, ezm, ex_jp, ez_jp, ey_ipw,
-                                                     ez_ipw, xsh, yzh, a, i0, j, km, sp, ij0, nxy, dx, div, hb);
+                                                     ez_ipw, xsh, yzh, ptab, a, i0, sp, ij0, nxy, dx, div, hb);
+            else if (!yz_plane(km))
+                stream_h_quad<false, false, false, COH>(nhx, nhy, nhz, ex, ey, exm, eym, ezm, ex_jp, ez_jp, ey_ipw,
+                                                        ez_ipw, xsh, yzh, ptab, a, i0, sp, ij0, nxy, dx, div, hb);
             else
                 stream_h_quad<false, false, true, COH>(nhx, nhy, nhz, ex, ey, exm, eym, ezm, ex_jp, ez_jp, ey_ipw,
-                                                       ez_ipw, xsh, yzh, a, i0, j, km, sp, ij0, nxy, dx, div, hb);
+                                                       ez_ipw, xsh, yzh, ptab, a, i0, sp, ij0, nxy, dx, div, hb);
             const long long g = ij0 + nxy * km;
             stv<4>(a.f_out[3] + g, nhx);
             stv<4>(a.f_out[4] + g, nhy);
             stv<4>(a.f_out[5] + g, nhz);
-            if (CPML) stream_psi_store<2>(xsh, yzh, a, q, j, km, ij0, nxy, xw);
+            if (CPML && (xw || yz_plane(km))) stream_psi_store<2>(xsh, yzh, a, q, j, km, ij0, nxy, xw);
         }
         load_yz(it + 1);
     }

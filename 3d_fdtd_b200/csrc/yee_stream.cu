@@ -67,7 +67,7 @@ static size_t stream_smem_floats(int nx, int ty, bool lossy, int L)
 {
     const int NA = lossy ? 12 : 9;
     return ((size_t)kStreamStages * NA * (ty + 1) + 2 * kStreamStages + 6 * (size_t)(ty + 1)) * nx +
-           (size_t)kStreamStages * 4 * (ty + 1) * stream_xpsi_stride(L);
+           (size_t)kStreamStages * 4 * (ty + 1) * stream_xpsi_stride(L) + (L > 0 ? 36 * (size_t)L : 0);
 }
 
 // split items 0..n-1 of cost c[] into at most `parts` contiguous runs of at

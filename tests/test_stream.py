@@ -65,7 +65,8 @@ def test_stream_plan_covers_interior_once(fd, nx, ny, nz, L, lossy, nsm):
     assert threads % 32 == 0 and threads == (want + 31) // 32 * 32 and threads <= 384
     na = 12 if lossy else 9
     xw = (2 * L + 3) // 4 * 4   # staged x-slab auxiliaries per row, padded to 16 bytes
-    assert smem == ((3 * na * (ty + 1) + 6 + 6 * (ty + 1)) * nx + 3 * 4 * (ty + 1) * xw) * 4 <= SMEM_MAX
+    ptab = 3 * 6 * 2 * L        # slab-cell profiles: 3 axes x 6 profiles x 2L cells
+    assert smem == ((3 * na * (ty + 1) + 6 + 6 * (ty + 1)) * nx + 3 * 4 * (ty + 1) * xw + ptab) * 4 <= SMEM_MAX
     owned = np.zeros((nz, ny), dtype=np.int64)
     for j0, rows, k0, k1 in tiles:
         assert 1 <= rows <= ty and j0 >= 1 and j0 + rows <= ny - 1

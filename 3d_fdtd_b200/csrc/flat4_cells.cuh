@@ -26,9 +26,11 @@ template <int W> __device__ __forceinline__ Vf<W> ldv(const float *p)
     if constexpr (W == 4) {
         const float4 t = __ldg(reinterpret_cast<const float4 *>(p));
         r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
-    } else {
+    } else if constexpr (W == 2) {
         const float2 t = __ldg(reinterpret_cast<const float2 *>(p));
         r.v[0] = t.x; r.v[1] = t.y;
+    } else {
+        r.v[0] = __ldg(p);
     }
     return r;
 }
@@ -39,9 +41,11 @@ template <int W> __device__ __forceinline__ Vf<W> ldv_rw(const float *p)
     if constexpr (W == 4) {
         const float4 t = *reinterpret_cast<const float4 *>(p);
         r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
-    } else {
+    } else if constexpr (W == 2) {
         const float2 t = *reinterpret_cast<const float2 *>(p);
         r.v[0] = t.x; r.v[1] = t.y;
+    } else {
+        r.v[0] = *p;
     }
     return r;
 }
@@ -62,7 +66,8 @@ template <bool COH> __device__ __forceinline__ float ldf1(const float *p)
 template <int W> __device__ __forceinline__ void stv(float *p, const Vf<W> &x)
 {
     if constexpr (W == 4) *reinterpret_cast<float4 *>(p) = make_float4(x.v[0], x.v[1], x.v[2], x.v[3]);
-    else *reinterpret_cast<float2 *>(p) = make_float2(x.v[0], x.v[1]);
+    else if constexpr (W == 2) *reinterpret_cast<float2 *>(p) = make_float2(x.v[0], x.v[1]);
+    else *p = x.v[0];
 }
 
 template <int W> __device__ __forceinline__ Vf<W> fillv(float s)

@@ -8,9 +8,9 @@
 namespace fdtd {
 
 constexpr int kStreamStages = 3;
-// 12 warps: up to 168 registers a thread at one block per SM (warps take
-// registers in groups of 4, so 13 warps would leave only 128)
-constexpr int kStreamMaxThreads = 384;
+// 16 warps: up to 128 registers a thread at one block per SM (an SM's four
+// sub-partitions hold 16K registers each, a quarter of the warps each)
+constexpr int kStreamMaxThreads = 512;
 
 __device__ __forceinline__ void cp_async16(float *smem, const float *gmem)
 {
@@ -35,34 +35,42 @@ __device__ __forceinline__ void sts4(float *p, const Vf<4> &x)
 {
     *reinterpret_cast<float4 *>(p) = make_float4(x.v[0], x.v[1], x.v[2], x.v[3]);
 }
-
-// ---- CPML auxiliaries of one quad for one field (E: A0 = 0, H: A0 = 2).
-//      x-slab: per element, staged in shared memory with the plane (rows of
-//      2L values); y- and z-slab: contiguous in x, read from global memory.
-//      The 1-D profiles of the slab cells sit in a shared table filled at the
-//      start of the tile (stream_profile_table): read from global memory at
-//      every use they missed L1 (the staged planes leave it a few KB) and put
-//      an L2 round trip on every x-slab cell's update.
-struct XPsi {
-    bool valid[4];
-    float p0[4], p1[4];
-};
-struct YZPsi {
-    int sj, sk;
-    Vf<4> pxy, pzy, pxz, pyz;   // as YZSlab: (x,y) (z,y) (x,z) (y,z) for E, alike for H
-};
-
-// x-slab auxiliaries of the quad from a staged row pair (row0, row1: the two
-// auxiliaries of this field for the cell row)
-__device__ __forceinline__ void stream_xpsi(XPsi &xs, const float *row0, const float *row1, int nx, int L, int q)
+__device__ __forceinline__ Vf<2> lds2(const float *p)
 {
-    const int i0 = 4 * q;
-    const bool any = i0 < L || i0 + 3 >= nx - L;
+    const float2 t = *reinterpret_cast<const float2 *>(p);
+    Vf<2> r;
+    r.v[0] = t.x; r.v[1] = t.y;
+    return r;
+}
+__device__ __forceinline__ void sts2(float *p, const Vf<2> &x) { *reinterpret_cast<float2 *>(p) = make_float2(x.v[0], x.v[1]); }
+
+// ---- CPML auxiliaries of one group of W consecutive x cells (an interior
+//      quad, W = 4, or one x-slab cell, W = 1) for one field (E: A0 = 0, H:
+//      A0 = 2).  x-slab: per element, staged in shared memory with the plane
+//      (rows of 2L values); y- and z-slab: contiguous in x, read from global
+//      memory.  The 1-D profiles of the slab cells sit in a shared table filled
+//      at the start of the tile (stream_profile_table): read from global
+//      memory at every use they missed L1 (the staged planes leave it a few
+//      KB) and put an L2 round trip on every x-slab cell's update.
+template <int W> struct XPsi {
+    bool valid[W];
+    float p0[W], p1[W];
+};
+template <int W> struct YZPsi {
+    int sj, sk;
+    Vf<W> pxy, pzy, pxz, pyz;   // as YZSlab: (x,y) (z,y) (x,z) (y,z) for E, alike for H
+};
+
+// x-slab auxiliaries of the group at x = i0.. from a staged row pair (row0,
+// row1: the two auxiliaries of this field for the cell row)
+template <int W>
+__device__ __forceinline__ void stream_xpsi(XPsi<W> &xs, const float *row0, const float *row1, int nx, int L, int i0)
+{
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
+    for (int e = 0; e < W; e++) {
         const int i = i0 + e;
         const int si = slab_local(i, nx, L);
-        xs.valid[e] = any && si >= 0 && i >= 1 && i <= nx - 2;
+        xs.valid[e] = si >= 0 && i >= 1 && i <= nx - 2;
         xs.p0[e] = xs.valid[e] ? row0[si] : 0.f;
         xs.p1[e] = xs.valid[e] ? row1[si] : 0.f;
     }
@@ -88,47 +96,45 @@ __device__ __forceinline__ void stream_profile_table(float *pt, const StreamArgs
 
 // COH: plain (coherent) loads, for launches in which other blocks wrote the
 // auxiliaries (the multi-step sweep); else the read-only path
-template <int A0, bool COH>
-__device__ __forceinline__ void stream_yzpsi_load(YZPsi &s, const StreamArgs &a, int q, int j, int k, long long ij0,
-                                                  long long nxy)
+template <int W, int A0, bool COH>
+__device__ __forceinline__ void stream_yzpsi_load(YZPsi<W> &s, const StreamArgs &a, int i0, int j, int k,
+                                                  long long ij0, long long nxy)
 {
-    const int nx = a.nx, L = a.L, i0 = 4 * q;
+    const int nx = a.nx, L = a.L;
     s.sj = slab_local(j, a.ny, L);
     s.sk = slab_local(k, a.nz, L);
-    s.pxy = fillv<4>(0.f); s.pzy = s.pxy; s.pxz = s.pxy; s.pyz = s.pxy;
+    s.pxy = fillv<W>(0.f); s.pzy = s.pxy; s.pxz = s.pxy; s.pyz = s.pxy;
     if (s.sj >= 0) {
         const long long sy = (long long)i0 + (long long)nx * (s.sj + 2LL * L * k);
-        s.pxy = ldf<4, COH>(a.psi_in[1][A0] + sy);
-        s.pzy = ldf<4, COH>(a.psi_in[1][A0 + 1] + sy);
+        s.pxy = ldf<W, COH>(a.psi_in[1][A0] + sy);
+        s.pzy = ldf<W, COH>(a.psi_in[1][A0 + 1] + sy);
     }
     if (s.sk >= 0) {
         const long long sz = ij0 + nxy * s.sk;
-        s.pxz = ldf<4, COH>(a.psi_in[2][A0] + sz);
-        s.pyz = ldf<4, COH>(a.psi_in[2][A0 + 1] + sz);
+        s.pxz = ldf<W, COH>(a.psi_in[2][A0] + sz);
+        s.pyz = ldf<W, COH>(a.psi_in[2][A0 + 1] + sz);
     }
 }
 
 // a quad wholly inside one x slab, with its auxiliaries 16-byte aligned (L
-// even): moved as one vector; the elements x = 0 / nx-1 hold 0, which is their
-// auxiliaries' value for good (they are never updated)
+// even): copied as one vector; the elements x = 0 / nx-1 hold 0, which is
+// their auxiliaries' value for good (they are never updated)
 __device__ __forceinline__ bool xquad_whole(int i0, int nx, int L)
 {
     return (L & 1) == 0 && (i0 + 3 < L || i0 >= nx - L);
 }
 
-template <int A0>
-__device__ __forceinline__ void stream_psi_store(const XPsi &xs, const YZPsi &s, const StreamArgs &a, int q, int j,
-                                                 int k, long long ij0, long long nxy, bool xquad)
+// updated auxiliaries of the group: x slab (XS: the group may hold x-slab
+// cells), then y and z slabs
+template <int W, int A0, bool XS>
+__device__ __forceinline__ void stream_psi_store(const XPsi<W> &xs, const YZPsi<W> &s, const StreamArgs &a, int i0,
+                                                 int j, int k, long long ij0, long long nxy)
 {
-    const int nx = a.nx, L = a.L, i0 = 4 * q;
-    const long long s0 = 2LL * L * (j + (long long)a.ny * k);
-    if (xquad && xquad_whole(i0, nx, L)) {
-        const long long si = s0 + slab_local(i0, nx, L);
-        *reinterpret_cast<float4 *>(a.psi_out[0][A0] + si) = make_float4(xs.p0[0], xs.p0[1], xs.p0[2], xs.p0[3]);
-        *reinterpret_cast<float4 *>(a.psi_out[0][A0 + 1] + si) = make_float4(xs.p1[0], xs.p1[1], xs.p1[2], xs.p1[3]);
-    } else if (xquad) {
+    const int nx = a.nx, L = a.L;
+    if (XS) {
+        const long long s0 = 2LL * L * (j + (long long)a.ny * k);
 #pragma unroll
-        for (int e = 0; e < 4; e++) {
+        for (int e = 0; e < W; e++) {
             if (!xs.valid[e]) continue;
             const long long sidx = s0 + slab_local(i0 + e, nx, L);
             a.psi_out[0][A0][sidx] = xs.p0[e];
@@ -137,13 +143,13 @@ __device__ __forceinline__ void stream_psi_store(const XPsi &xs, const YZPsi &s,
     }
     if (s.sj >= 0) {
         const long long sy = (long long)i0 + (long long)nx * (s.sj + 2LL * L * k);
-        stv<4>(a.psi_out[1][A0] + sy, s.pxy);
-        stv<4>(a.psi_out[1][A0 + 1] + sy, s.pzy);
+        stv<W>(a.psi_out[1][A0] + sy, s.pxy);
+        stv<W>(a.psi_out[1][A0 + 1] + sy, s.pzy);
     }
     if (s.sk >= 0) {
         const long long sz = ij0 + nxy * s.sk;
-        stv<4>(a.psi_out[2][A0] + sz, s.pxz);
-        stv<4>(a.psi_out[2][A0 + 1] + sz, s.pyz);
+        stv<W>(a.psi_out[2][A0] + sz, s.pxz);
+        stv<W>(a.psi_out[2][A0 + 1] + sz, s.pyz);
     }
 }
 
@@ -153,8 +159,8 @@ __device__ __forceinline__ void stream_psi_store(const XPsi &xs, const YZPsi &s,
 // H.  X: the cell may lie in an x slab (its x terms are compiled in); without
 // X the x terms are the interior's (kappa 1, no auxiliary), exactly what the
 // general expression gives there.
-template <bool X, int pw>
-__device__ __forceinline__ Curl3 stream_cpml_curl(XPsi &xs, YZPsi &s, const float *pt, int nx, int L, int i, int e,
+template <int W, bool X, int pw>
+__device__ __forceinline__ Curl3 stream_cpml_curl(XPsi<W> &xs, YZPsi<W> &s, const float *pt, int nx, int L, int i, int e,
                                                   float d_zy, float d_yz, float d_xz, float d_zx, float d_yx,
                                                   float d_xy, float dx, float div)
 {
@@ -202,15 +208,19 @@ __device__ __forceinline__ void cp_async4(float *smem, const float *gmem)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
-// Work roles of the block's threads.  Each thread owns 4 consecutive x cells
-// (a quad) of one staged row.  On a CPML grid the quads that reach into an x
-// slab (row ends) sit in warps of their own, after the interior quads, so the
-// x-slab work never diverges inside an interior warp and interior warps carry
-// no x-slab code at all.
+// Work roles of the block's threads.  An interior thread owns 4 consecutive x
+// cells (a quad) of one staged row.  On a CPML grid the quads that reach into
+// an x slab (row ends) are not given to quad threads: every cell of them has
+// a thread of its own (x-cell threads, 4 consecutive lanes per quad), in
+// warps after the interior ones.  An x-slab cell's update carries the
+// auxiliary recursion, its profiles and the row-end rules, several times the
+// work of an interior cell, and the block waits for its slowest warp at each
+// plane's barrier: a whole quad per thread (or a pair) made the x-slab
+// threads the slowest of every plane.  Interior warps carry no x-slab code.
 struct StreamRoles {
     int QL, QR;      // x-slab quads: q < QL or q >= QR (QL = QR = 0 when there is no x slab)
     int QI, NXQ;     // interior and x-slab quads per row
-    int xbase;       // first thread of the x-slab warps
+    int xbase;       // first thread of the x-cell warps
     int threads;     // block size
 };
 
@@ -231,29 +241,30 @@ __host__ __device__ inline StreamRoles stream_roles(int nx, int L, int tp)
     r.QI = r.QR - r.QL;
     r.NXQ = QX - r.QI;
     r.xbase = (tp * r.QI + 31) / 32 * 32;
-    r.threads = (r.xbase + tp * r.NXQ + 31) / 32 * 32;
+    r.threads = (r.xbase + tp * 4 * r.NXQ + 31) / 32 * 32;
     return r;
 }
 
-// E_new of one quad.  X: x-slab quad (x terms, and the cells x = 0 / nx-1 of
-// the row ends stay); EDGE: the quad may hold x = 0 / nx-1 (row ends of a grid
-// without CPML).
-template <bool X, bool EDGE, bool CPML, bool LOSSY, bool COH>
-__device__ __forceinline__ void stream_e_quad(Vf<4> &ex, Vf<4> &ey, Vf<4> &ez, const Vf<4> &hx, const Vf<4> &hy,
-                                              const Vf<4> &hz, const Vf<4> &hx_km, const Vf<4> &hy_km,
-                                              const Vf<4> &hx_jm, const Vf<4> &hz_jm, float hy_im0, float hz_im0,
-                                              const Vf<4> &b0, const Vf<4> &b1, const Vf<4> &b2, const Vf<4> &c0,
-                                              const Vf<4> &c1, const Vf<4> &c2, XPsi &xs, YZPsi &yz,
-                                              const float *pt, const StreamArgs &a, int i0, const float *sp,
-                                              long long ij0, long long nxy, float dx, float div)
+// E_new of one group of W cells at x = i0 (an interior quad, W = 4, or one
+// x-slab cell, W = 1).  X: x-slab group (x terms, and the cells x = 0 / nx-1
+// of the row ends stay); EDGE: the group may hold x = 0 / nx-1 (row ends of a
+// grid without CPML).  hy_im0, hz_im0: Hy, Hz at x = i0 - 1.
+template <int W, bool X, bool EDGE, bool CPML, bool LOSSY, bool COH>
+__device__ __forceinline__ void stream_e_group(Vf<W> &ex, Vf<W> &ey, Vf<W> &ez, const Vf<W> &hx, const Vf<W> &hy,
+                                               const Vf<W> &hz, const Vf<W> &hx_km, const Vf<W> &hy_km,
+                                               const Vf<W> &hx_jm, const Vf<W> &hz_jm, float hy_im0, float hz_im0,
+                                               const Vf<W> &b0, const Vf<W> &b1, const Vf<W> &b2, const Vf<W> &c0,
+                                               const Vf<W> &c1, const Vf<W> &c2, XPsi<W> &xs, YZPsi<W> &yz,
+                                               const float *pt, const StreamArgs &a, int i0, const float *sp,
+                                               long long ij0, long long nxy, float dx, float div)
 {
     const bool plain = !CPML || (!X && yz.sj < 0 && yz.sk < 0);
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
+    for (int e = 0; e < W; e++) {
         const int i = i0 + e;
         if ((X || EDGE) && (i < 1 || i > a.nx - 2)) continue;   // x = 0 and x = nx-1 stay
-        const float hy_im = e == 0 ? hy_im0 : hy.v[e - 1];
-        const float hz_im = e == 0 ? hz_im0 : hz.v[e - 1];
+        const float hy_im = e == 0 ? hy_im0 : hy.v[e == 0 ? 0 : e - 1];
+        const float hz_im = e == 0 ? hz_im0 : hz.v[e == 0 ? 0 : e - 1];
         const float dHz_dy = hz.v[e] - hz_jm.v[e];
         const float dHy_dz = hy.v[e] - hy_km.v[e];
         const float dHx_dz = hx.v[e] - hx_km.v[e];
@@ -266,8 +277,8 @@ __device__ __forceinline__ void stream_e_quad(Vf<4> &ex, Vf<4> &ey, Vf<4> &ez, c
             cy = dHx_dz - dHz_dx;
             cz = dHy_dx - dHx_dy;
         } else {
-            const Curl3 c = stream_cpml_curl<X, 0>(xs, yz, pt, a.nx, a.L, i, e, dHz_dy, dHy_dz, dHx_dz, dHz_dx,
-                                                   dHy_dx, dHx_dy, dx, div);
+            const Curl3 c = stream_cpml_curl<W, X, 0>(xs, yz, pt, a.nx, a.L, i, e, dHz_dy, dHy_dz, dHx_dz, dHz_dx,
+                                                      dHy_dx, dHx_dy, dx, div);
             cx = c.x; cy = c.y; cz = c.z;
         }
         if (sp) {
@@ -281,22 +292,23 @@ __device__ __forceinline__ void stream_e_quad(Vf<4> &ex, Vf<4> &ey, Vf<4> &ez, c
     }
 }
 
-// H_new of one quad (same roles as stream_e_quad)
-template <bool X, bool EDGE, bool CPML, bool COH>
-__device__ __forceinline__ void stream_h_quad(Vf<4> &nhx, Vf<4> &nhy, Vf<4> &nhz, const Vf<4> &ex, const Vf<4> &ey,
-                                              const Vf<4> &exm, const Vf<4> &eym, const Vf<4> &ezm,
-                                              const Vf<4> &ex_jp, const Vf<4> &ez_jp, float ey_ipw, float ez_ipw,
-                                              XPsi &xs, YZPsi &yz, const float *pt, const StreamArgs &a, int i0,
-                                              const float *sp, long long ij0, long long nxy, float dx, float div,
-                                              float hb)
+// H_new of one group (same roles as stream_e_group); ey_ipw, ez_ipw: new Ey,
+// Ez at x = i0 + W
+template <int W, bool X, bool EDGE, bool CPML, bool COH>
+__device__ __forceinline__ void stream_h_group(Vf<W> &nhx, Vf<W> &nhy, Vf<W> &nhz, const Vf<W> &ex, const Vf<W> &ey,
+                                               const Vf<W> &exm, const Vf<W> &eym, const Vf<W> &ezm,
+                                               const Vf<W> &ex_jp, const Vf<W> &ez_jp, float ey_ipw, float ez_ipw,
+                                               XPsi<W> &xs, YZPsi<W> &yz, const float *pt, const StreamArgs &a,
+                                               int i0, const float *sp, long long ij0, long long nxy, float dx,
+                                               float div, float hb)
 {
     const bool plain = !CPML || (!X && yz.sj < 0 && yz.sk < 0);
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
+    for (int e = 0; e < W; e++) {
         const int i = i0 + e;
         if ((X || EDGE) && (i < 1 || i > a.nx - 2)) continue;
-        const float ey_ip = e == 3 ? ey_ipw : eym.v[e + 1];
-        const float ez_ip = e == 3 ? ez_ipw : ezm.v[e + 1];
+        const float ey_ip = e == W - 1 ? ey_ipw : eym.v[e == W - 1 ? e : e + 1];
+        const float ez_ip = e == W - 1 ? ez_ipw : ezm.v[e == W - 1 ? e : e + 1];
         const float dEz_dy = ez_jp.v[e] - ezm.v[e];
         const float dEy_dz = ey.v[e] - eym.v[e];
         const float dEx_dz = ex.v[e] - exm.v[e];
@@ -309,8 +321,8 @@ __device__ __forceinline__ void stream_h_quad(Vf<4> &nhx, Vf<4> &nhy, Vf<4> &nhz
             cy = dEx_dz - dEz_dx;
             cz = dEy_dx - dEx_dy;
         } else {
-            const Curl3 c = stream_cpml_curl<X, 3>(xs, yz, pt, a.nx, a.L, i, e, dEz_dy, dEy_dz, dEx_dz, dEz_dx,
-                                                   dEy_dx, dEx_dy, dx, div);
+            const Curl3 c = stream_cpml_curl<W, X, 3>(xs, yz, pt, a.nx, a.L, i, e, dEz_dy, dEy_dz, dEx_dz, dEz_dx,
+                                                      dEy_dx, dEx_dy, dx, div);
             cx = c.x; cy = c.y; cz = c.z;
         }
         if (sp) {
@@ -324,9 +336,23 @@ __device__ __forceinline__ void stream_h_quad(Vf<4> &nhx, Vf<4> &nhy, Vf<4> &nhz
     }
 }
 
+// The tile's per-plane barrier.  The two thread roles run loops of their own
+// (each with the registers of its own work only) and meet here once per
+// iteration, the same number of times: every thread of the block takes part.
+__device__ __forceinline__ void stream_plane_barrier() { asm volatile("bar.sync 1;\n" ::: "memory"); }
+
 // One tile (band of rows x chunk of planes) of one grid's step, by the whole
 // block, with `sm` the block's dynamic shared memory (stream_smem_floats of
 // the grid's nx, a.ty, loss and L).  Ends with no copy in flight.
+//
+// Iteration it (plane k = k0 + it, it = 0..n) updates E of plane k (owned rows
+// and the halo row j0 + rows) and H of plane k-1 (owned rows), with the
+// staged planes of a 3-stage ring: stage it % 3 holds plane k, the previous
+// stage plane k-1, and right after the barrier the previous stage takes the
+// copies of plane k+2.  Each thread copies only slots that it reads itself in
+// the iteration that refills them (old H of plane k-1, H's x-slab
+// auxiliaries); the four x-cell lanes of a quad read their elements of slots
+// that another of them copies, so they meet at a warp barrier in between.
 template <bool CPML, bool LOSSY, bool COH = false>
 __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTile tl, float *sm)
 {
@@ -336,216 +362,351 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
     const int TP = a.ty + 1;                         // staged rows per array
     const int XW = stream_xpsi_stride(L);            // staged x-slab auxiliaries per row (2L, padded)
     const long long nxy = (long long)nx * ny;
-    // thread -> (staged row r, quad q); r = TP marks an idle thread
     const StreamRoles ro = stream_roles(nx, L, TP);
     const int tid = (int)threadIdx.x;
     const bool xw = CPML && tid >= ro.xbase;          // warp-uniform: xbase is a multiple of 32
-    int r, q;
-    if (!xw) {
-        r = tid < TP * ro.QI ? tid / ro.QI : TP;
-        q = r < TP ? ro.QL + (tid - r * ro.QI) : 0;
-    } else {
-        const int u = tid - ro.xbase;
-        r = u < TP * ro.NXQ ? u / ro.NXQ : TP;
-        const int v = r < TP ? u - r * ro.NXQ : 0;
-        q = v < ro.QL ? v : ro.QR + (v - ro.QL);
-    }
     const int R = tl.rows;
-    const bool act = r <= R;                         // owned row (r < R) or the halo row (r == R)
-    const bool own = r < R;
-    const int j = tl.j0 + r;
-    const int i0 = 4 * q;
     const int QX = nx >> 2;
-    const long long ij0 = (long long)i0 + (long long)nx * j;
     float *stage = sm;                               // [S][NA][TP][nx]
     float *xps = stage + (size_t)S * NA * TP * nx;   // [S][4][TP][XW]: x-slab auxiliaries E0 E1 H0 H1
     float *hlow = xps + (size_t)S * 4 * TP * XW;     // [S][2][nx]: Hx, Hz of row j0-1
     float *es = hlow + (size_t)S * 2 * nx;           // [2][3][TP][nx]: new E of the last two planes
     float *ptab = es + (size_t)2 * 3 * TP * nx;      // CPML profiles of the slab cells (stream_profile_table)
     if (CPML) stream_profile_table(ptab, a);
-    auto stg = [&](int s, int arr, int row) -> float * { return stage + ((size_t)(s * NA + arr) * TP + row) * nx; };
-    auto xrow = [&](int s, int arr, int row) -> float * { return xps + ((size_t)(s * 4 + arr) * TP + row) * XW; };
-    auto esp = [&](int b, int c, int row) -> float * { return es + ((size_t)(b * 3 + c) * TP + row) * nx; };
+    // shared-memory offsets fit 32 bits (the whole allocation is < 64K floats)
+    auto stg = [&](int s, int arr, int row) -> float * { return stage + ((s * NA + arr) * TP + row) * nx; };
+    auto xrow = [&](int s, int arr, int row) -> float * { return xps + ((s * 4 + arr) * TP + row) * XW; };
+    auto esp = [&](int b, int c, int row) -> float * { return es + ((b * 3 + c) * TP + row) * nx; };
+    auto hlw = [&](int s, int c) -> float * { return hlow + (s * 2 + c) * nx; };
     const int n = tl.k1 - tl.k0;                     // owned planes; iterations 0..n
+    const float dx = a.dx, div = 1.0f / dx, hb = a.hb;
+    // z-slab planes (block-uniform); with the y-slab rows (per thread, and
+    // warp-uniform but for the warps that hold a band's last rows) they are
+    // where a cell carries y or z auxiliaries: elsewhere interior quads run
+    // the plain updates, with no auxiliary state; the general CPML expression
+    // computes the same values there (kappa 1, no auxiliaries).
+    auto z_plane = [&](int k) { return CPML && (k < L || k >= nz - L); };
 
-    // Copies of iteration `it` (plane k0 + it) into stage (it + S) % S, one
-    // group per call.  Every thread copies only its own slots (row r, quad q;
-    // row 0 also the j0-1 slots; an x-slab quad its elements' auxiliaries),
-    // and other threads read those slots only in the iteration that consumes
-    // the stage, after the barrier that follows the copy.  `h_only`: just H
-    // (iteration -1, plane k0 - 1: the previous plane of iteration 0).
-    auto issue = [&](int it, bool h_only) {
-        if (it <= n && act) {
-            const int s = (it + S) % S;
-            const int k = tl.k0 + it;
-            const long long g = ij0 + nxy * k;
+    if (!xw) {
+        // ---- interior quads (every quad of a grid without CPML); r = TP: idle
+        const int r = tid < TP * ro.QI ? tid / ro.QI : TP;
+        const int q = r < TP ? ro.QL + (tid - r * ro.QI) : 0;
+        const bool act = r <= R;                     // owned row (r < R) or the halo row (r == R)
+        const bool own = r < R;
+        const int j = tl.j0 + r, i0 = 4 * q;
+        const long long ij0 = (long long)i0 + (long long)nx * j;
+        const bool row_upd = j >= 1 && j <= ny - 2;  // false only for a halo row on the shell
+        const bool y_row = CPML && (j < L || j >= ny - L);
+        auto yz_plane = [&](int k) { return y_row || z_plane(k); };
+        // copies of iteration `it` (plane k0 + it) into stage (it + S) % S, one
+        // group per call; `h_only`: just H (iteration -1, plane k0 - 1)
+        auto issue = [&](int it, bool h_only) {
+            if (it <= n && act) {
+                const int s = (it + S) % S;
+                const long long g = ij0 + nxy * (tl.k0 + it);
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                cp_async16(stg(s, c, r) + i0, a.f_in[3 + c] + g);
-                if (!h_only) {
-                    cp_async16(stg(s, 3 + c, r) + i0, a.f_in[c] + g);
-                    cp_async16(stg(s, 6 + c, r) + i0, a.cb[c] + g);
-                    if (LOSSY) cp_async16(stg(s, 9 + c, r) + i0, a.ca[c] + g);
+                for (int c = 0; c < 3; c++) {
+                    cp_async16(stg(s, c, r) + i0, a.f_in[3 + c] + g);
+                    if (!h_only) {
+                        cp_async16(stg(s, 3 + c, r) + i0, a.f_in[c] + g);
+                        cp_async16(stg(s, 6 + c, r) + i0, a.cb[c] + g);
+                        if (LOSSY) cp_async16(stg(s, 9 + c, r) + i0, a.ca[c] + g);
+                    }
+                }
+                if (r == 0 && !h_only) {
+                    cp_async16(hlw(s, 0) + i0, a.f_in[3] + g - nx);
+                    cp_async16(hlw(s, 1) + i0, a.f_in[5] + g - nx);
                 }
             }
-            if (r == 0 && !h_only) {
-                cp_async16(hlow + (size_t)(s * 2 + 0) * nx + i0, a.f_in[3] + g - nx);
-                cp_async16(hlow + (size_t)(s * 2 + 1) * nx + i0, a.f_in[5] + g - nx);
+            cp_async_commit_group();
+        };
+        issue(-1, true);
+        issue(0, false);
+        issue(1, false);
+        // y- and z-slab auxiliaries of iteration `it`'s updates (E of plane k,
+        // H of plane k-1), read from global memory one iteration ahead
+        YZPsi<4> yze, yzh;
+        auto load_yz = [&](int it) {
+            yze.sj = yze.sk = yzh.sj = yzh.sk = -1;
+            if (!CPML || it > n) return;
+            const int k = tl.k0 + it;
+            if (!yz_plane(k) && !yz_plane(k - 1)) return;
+            if (act && row_upd && k <= nz - 2) stream_yzpsi_load<4, 0, COH>(yze, a, i0, j, k, ij0, nxy);
+            if (own && it >= 1) stream_yzpsi_load<4, 2, COH>(yzh, a, i0, j, k - 1, ij0, nxy);
+        };
+        load_yz(0);
+        XPsi<4> xnone;                               // interior quads hold no x-slab cell
+#pragma unroll
+        for (int e = 0; e < 4; e++) { xnone.valid[e] = false; xnone.p0[e] = xnone.p1[e] = 0.f; }
+
+        for (int it = 0; it <= n; it++) {
+            const int k = tl.k0 + it;
+            const int s = it % S, sp_ = (it + S - 1) % S;      // this plane's stage, the previous plane's
+            const bool e_upd = act && row_upd && k <= nz - 2;   // k >= 1 always
+            const bool h_upd = own && it >= 1;
+            cp_async_wait_group<1>();   // this thread's copies up to iteration it have landed
+            stream_plane_barrier();     // ... and everyone's; new E of iteration it-1 visible
+            // own slots of the previous plane's stage: old H (the E update's z
+            // neighbours, the H update's base value); then that stage takes
+            // plane it+2
+            Vf<4> hxm = fillv<4>(0.f), hym = hxm, hzm = hxm;
+            if (act) {
+                hxm = lds4(stg(sp_, 0, r) + i0);
+                hym = lds4(stg(sp_, 1, r) + i0);
+                hzm = lds4(stg(sp_, 2, r) + i0);
             }
-            if (CPML && xw && !h_only) {
-                const long long xs0 = 2LL * L * (j + (long long)ny * k);
-                const int si0 = slab_local(i0, nx, L);
-                if (xquad_whole(i0, nx, L)) {
-                    // the quad lies in one slab and its 4 auxiliaries are 16-byte aligned
+            issue(it + 2, false);
+
+            // ---- E_new(k) of rows j0..j0+R
+            Vf<4> ex = fillv<4>(0.f), ey = ex, ez = ex;
+            if (act) {
+                ex = lds4(stg(s, 3, r) + i0);
+                ey = lds4(stg(s, 4, r) + i0);
+                ez = lds4(stg(s, 5, r) + i0);
+            }
+            if (e_upd) {
+                const Vf<4> hx = lds4(stg(s, 0, r) + i0), hy = lds4(stg(s, 1, r) + i0), hz = lds4(stg(s, 2, r) + i0);
+                const Vf<4> hx_jm = lds4((r > 0 ? stg(s, 0, r - 1) : hlw(s, 0)) + i0);
+                const Vf<4> hz_jm = lds4((r > 0 ? stg(s, 2, r - 1) : hlw(s, 1)) + i0);
+                const float hy_im0 = q > 0 ? stg(s, 1, r)[i0 - 1] : 0.f;
+                const float hz_im0 = q > 0 ? stg(s, 2, r)[i0 - 1] : 0.f;
+                const Vf<4> b0 = lds4(stg(s, 6, r) + i0), b1 = lds4(stg(s, 7, r) + i0), b2 = lds4(stg(s, 8, r) + i0);
+                Vf<4> c0 = fillv<4>(1.f), c1 = c0, c2 = c0;
+                if (LOSSY) {
+                    c0 = lds4(stg(s, 9, r) + i0);
+                    c1 = lds4(stg(s, 10, r) + i0);
+                    c2 = lds4(stg(s, 11, r) + i0);
+                }
+                const float *sp = a.src.n ? src_plane(a.src, k) : nullptr;
+                if (!CPML)
+                    stream_e_group<4, false, true, false, LOSSY, COH>(ex, ey, ez, hx, hy, hz, hxm, hym, hx_jm, hz_jm,
+                                                                      hy_im0, hz_im0, b0, b1, b2, c0, c1, c2, xnone,
+                                                                      yze, ptab, a, i0, sp, ij0, nxy, dx, div);
+                else if (!yz_plane(k))
+                    stream_e_group<4, false, false, false, LOSSY, COH>(ex, ey, ez, hx, hy, hz, hxm, hym, hx_jm,
+                                                                       hz_jm, hy_im0, hz_im0, b0, b1, b2, c0, c1, c2,
+                                                                       xnone, yze, ptab, a, i0, sp, ij0, nxy, dx,
+                                                                       div);
+                else
+                    stream_e_group<4, false, false, true, LOSSY, COH>(ex, ey, ez, hx, hy, hz, hxm, hym, hx_jm, hz_jm,
+                                                                      hy_im0, hz_im0, b0, b1, b2, c0, c1, c2, xnone,
+                                                                      yze, ptab, a, i0, sp, ij0, nxy, dx, div);
+            }
+            if (act) {
+                const int b = it & 1;
+                sts4(esp(b, 0, r) + i0, ex);
+                sts4(esp(b, 1, r) + i0, ey);
+                sts4(esp(b, 2, r) + i0, ez);
+            }
+            if (own && it < n) {
+                const long long g = ij0 + nxy * k;
+                stv<4>(a.f_out[0] + g, ex);
+                stv<4>(a.f_out[1] + g, ey);
+                stv<4>(a.f_out[2] + g, ez);
+                if (CPML && yz_plane(k)) stream_psi_store<4, 0, false>(xnone, yze, a, i0, j, k, ij0, nxy);
+            }
+
+            // ---- H_new(k-1) of rows j0..j0+R-1: own old H from the previous
+            //      stage, the new E of plane k-1 from the shared array of
+            //      iteration it-1 (own cells and neighbours), the new E of
+            //      plane k from registers
+            if (h_upd) {
+                const int km = k - 1;
+                const int b = (it - 1) & 1;
+                const Vf<4> exm = lds4(esp(b, 0, r) + i0), eym = lds4(esp(b, 1, r) + i0), ezm = lds4(esp(b, 2, r) + i0);
+                const Vf<4> ex_jp = lds4(esp(b, 0, r + 1) + i0), ez_jp = lds4(esp(b, 2, r + 1) + i0);
+                const float ey_ipw = q < QX - 1 ? esp(b, 1, r)[i0 + 4] : 0.f;
+                const float ez_ipw = q < QX - 1 ? esp(b, 2, r)[i0 + 4] : 0.f;
+                Vf<4> nhx = hxm, nhy = hym, nhz = hzm;
+                const float *sp = a.src.n ? src_plane(a.src, km) : nullptr;
+                if (!CPML)
+                    stream_h_group<4, false, true, false, COH>(nhx, nhy, nhz, ex, ey, exm, eym, ezm, ex_jp, ez_jp,
+                                                               ey_ipw, ez_ipw, xnone, yzh, ptab, a, i0, sp, ij0, nxy,
+                                                               dx, div, hb);
+                else if (!yz_plane(km))
+                    stream_h_group<4, false, false, false, COH>(nhx, nhy, nhz, ex, ey, exm, eym, ezm, ex_jp, ez_jp,
+                                                                ey_ipw, ez_ipw, xnone, yzh, ptab, a, i0, sp, ij0, nxy,
+                                                                dx, div, hb);
+                else
+                    stream_h_group<4, false, false, true, COH>(nhx, nhy, nhz, ex, ey, exm, eym, ezm, ex_jp, ez_jp,
+                                                               ey_ipw, ez_ipw, xnone, yzh, ptab, a, i0, sp, ij0, nxy,
+                                                               dx, div, hb);
+                const long long g = ij0 + nxy * km;
+                stv<4>(a.f_out[3] + g, nhx);
+                stv<4>(a.f_out[4] + g, nhy);
+                stv<4>(a.f_out[5] + g, nhz);
+                if (CPML && yz_plane(km)) stream_psi_store<4, 2, false>(xnone, yzh, a, i0, j, km, ij0, nxy);
+            }
+            load_yz(it + 1);
+        }
+        cp_async_wait_group<0>();
+        return;
+    }
+    if constexpr (CPML) {
+        // ---- x-slab cells, one per thread; the 4 lanes of a quad are
+        //      consecutive (NXC is a multiple of 4, xbase of 32) and share the
+        //      quad's 16-byte copies: lane e moves staged arrays e, e+4, e+8
+        //      (H0-2, E0-2, cb0-2, ca0-2 in that order), x-slab auxiliary e and,
+        //      on the band's first row, Hx (lane 0) or Hz (lane 1) of row
+        //      j0-1; r = TP: idle
+        const int NXC = 4 * ro.NXQ;
+        const int u = tid - ro.xbase;
+        const int r = u < TP * NXC ? u / NXC : TP;
+        const int cc = r < TP ? u - r * NXC : 0;
+        const int v = cc >> 2, e4 = cc & 3;
+        const int q = v < ro.QL ? v : ro.QR + (v - ro.QL);
+        const int i0 = 4 * q, i = i0 + e4;
+        const bool act = r <= R;
+        const bool own = r < R;
+        const int j = tl.j0 + r;
+        const long long ijq = (long long)i0 + (long long)nx * j;   // the quad's first cell
+        const long long ij = ijq + e4;                             // this thread's cell
+        const bool row_upd = j >= 1 && j <= ny - 2;
+        const bool y_row = j < L || j >= ny - L;
+        auto yz_plane = [&](int k) { return y_row || z_plane(k); };
+        const bool whole = xquad_whole(i0, nx, L);
+        const int si = slab_local(i, nx, L);
+        // source array of staged array `arr` (selects, no branches: the lanes of
+        // a warp take different arrays)
+        auto src_of = [&](int arr) -> const float * {
+            const int c = arr % 3;
+            const float *p = arr < 3 ? a.f_in[3 + c] : a.f_in[c];
+            if (arr >= 6) p = a.cb[c];
+            if (LOSSY && arr >= 9) p = a.ca[c];
+            return p;
+        };
+        auto issue = [&](int it, bool h_only) {
+            if (it <= n && act) {
+                const int s = (it + S) % S;
+                const int k = tl.k0 + it;
+                const long long g = ijq + nxy * k;
 #pragma unroll
-                    for (int arr = 0; arr < 4; arr++) cp_async16(xrow(s, arr, r) + si0, a.psi_in[0][arr] + xs0 + si0);
-                } else {
+                for (int m = 0; m < 3; m++) {
+                    const int arr = e4 + 4 * m;
+                    if (arr < (h_only ? 3 : NA)) cp_async16(stg(s, arr, r) + i0, src_of(arr) + g);
+                }
+                if (!h_only) {
+                    if (r == 0 && e4 < 2) cp_async16(hlw(s, e4) + i0, a.f_in[3 + 2 * e4] + g - nx);
+                    const long long xs0 = 2LL * L * (j + (long long)ny * k);
+                    if (whole) {
+                        // the quad lies in one slab and its 4 auxiliaries are 16-byte aligned
+                        const int si0 = slab_local(i0, nx, L);
+                        cp_async16(xrow(s, e4, r) + si0, a.psi_in[0][e4] + xs0 + si0);
+                    } else if (si >= 0) {
 #pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const int si = slab_local(i0 + e, nx, L);
-                        if (si < 0) continue;
-#pragma unroll
-                        for (int arr = 0; arr < 4; arr++)
-                            cp_async4(xrow(s, arr, r) + si, a.psi_in[0][arr] + xs0 + si);
+                        for (int arr = 0; arr < 4; arr++) cp_async4(xrow(s, arr, r) + si, a.psi_in[0][arr] + xs0 + si);
                     }
                 }
             }
-        }
-        cp_async_commit_group();
-    };
-    issue(-1, true);
-    issue(0, false);
-    issue(1, false);
-    const float dx = a.dx, div = 1.0f / dx, hb = a.hb;
-    const bool row_upd = j >= 1 && j <= ny - 2;      // false only for a halo row on the shell
-    // y- and z-slab auxiliaries of iteration `it`'s updates (E of plane k, H of
-    // plane k-1), read from global memory one iteration ahead
-    YZPsi yze, yzh;
-    // Iterations whose planes hold no y- or z-slab cell of the tile's rows
-    // (block-uniform): interior quads run the plain updates there, with no
-    // auxiliary state; the general CPML expression computes the same values
-    // there (kappa 1, no auxiliaries).
-    const bool y_rows = CPML && (tl.j0 < L || tl.j0 + R >= ny - L);
-    auto yz_plane = [&](int k) { return y_rows || (CPML && (k < L || k >= nz - L)); };
-    auto load_yz = [&](int it) {
-        yze.sj = yze.sk = yzh.sj = yzh.sk = -1;
-        if (!CPML || it > n) return;
-        const int k = tl.k0 + it;
-        if (!xw && !yz_plane(k) && !yz_plane(k - 1)) return;
-        if (act && row_upd && k <= nz - 2) stream_yzpsi_load<0, COH>(yze, a, q, j, k, ij0, nxy);
-        if (own && it >= 1) stream_yzpsi_load<2, COH>(yzh, a, q, j, k - 1, ij0, nxy);
-    };
-    load_yz(0);
+            cp_async_commit_group();
+        };
+        issue(-1, true);
+        issue(0, false);
+        issue(1, false);
+        YZPsi<1> yze, yzh;
+        auto load_yz = [&](int it) {
+            yze.sj = yze.sk = yzh.sj = yzh.sk = -1;
+            if (it > n) return;
+            const int k = tl.k0 + it;
+            if (!yz_plane(k) && !yz_plane(k - 1)) return;
+            if (act && row_upd && k <= nz - 2) stream_yzpsi_load<1, 0, COH>(yze, a, i, j, k, ij, nxy);
+            if (own && it >= 1) stream_yzpsi_load<1, 2, COH>(yzh, a, i, j, k - 1, ij, nxy);
+        };
+        load_yz(0);
 
-    for (int it = 0; it <= n; it++) {
-        const int k = tl.k0 + it;
-        const int s = it % S, sp_ = (it + S - 1) % S;      // this plane's stage, the previous plane's
-        const bool e_upd = act && row_upd && k <= nz - 2;   // k >= 1 always
-        const bool h_upd = own && it >= 1;
-        cp_async_wait_group<1>();   // this thread's copies up to iteration it have landed
-        __syncthreads();            // ... and everyone's; new E of iteration it-1 visible
-        // own slots of the previous plane's stage: old H (the E update's z
-        // neighbours, the H update's base value) and the H update's x-slab
-        // auxiliaries; then that stage takes plane it+2 (other threads read
-        // these slots only in iteration it-1, which every thread has left)
-        Vf<4> hxm = fillv<4>(0.f), hym = hxm, hzm = hxm;
-        if (act) {
-            hxm = lds4(stg(sp_, 0, r) + i0);
-            hym = lds4(stg(sp_, 1, r) + i0);
-            hzm = lds4(stg(sp_, 2, r) + i0);
-        }
-        XPsi xsh;
-        if (CPML && xw && h_upd) stream_xpsi(xsh, xrow(sp_, 2, r), xrow(sp_, 3, r), nx, L, q);
-        issue(it + 2, false);
-
-        // ---- E_new(k) of rows j0..j0+R
-        Vf<4> ex = fillv<4>(0.f), ey = ex, ez = ex;
-        if (act) {
-            ex = lds4(stg(s, 3, r) + i0);
-            ey = lds4(stg(s, 4, r) + i0);
-            ez = lds4(stg(s, 5, r) + i0);
-        }
-        XPsi xse;
-        if (e_upd) {
-            if (CPML && xw) stream_xpsi(xse, xrow(s, 0, r), xrow(s, 1, r), nx, L, q);
-            const Vf<4> hx = lds4(stg(s, 0, r) + i0), hy = lds4(stg(s, 1, r) + i0), hz = lds4(stg(s, 2, r) + i0);
-            const Vf<4> hx_jm = r > 0 ? lds4(stg(s, 0, r - 1) + i0) : lds4(hlow + (size_t)(s * 2 + 0) * nx + i0);
-            const Vf<4> hz_jm = r > 0 ? lds4(stg(s, 2, r - 1) + i0) : lds4(hlow + (size_t)(s * 2 + 1) * nx + i0);
-            const float hy_im0 = q > 0 ? stg(s, 1, r)[i0 - 1] : 0.f;
-            const float hz_im0 = q > 0 ? stg(s, 2, r)[i0 - 1] : 0.f;
-            const Vf<4> b0 = lds4(stg(s, 6, r) + i0), b1 = lds4(stg(s, 7, r) + i0), b2 = lds4(stg(s, 8, r) + i0);
-            Vf<4> c0 = fillv<4>(1.f), c1 = c0, c2 = c0;
-            if (LOSSY) {
-                c0 = lds4(stg(s, 9, r) + i0);
-                c1 = lds4(stg(s, 10, r) + i0);
-                c2 = lds4(stg(s, 11, r) + i0);
+        for (int it = 0; it <= n; it++) {
+            const int k = tl.k0 + it;
+            const int s = it % S, sp_ = (it + S - 1) % S;
+            const bool e_upd = act && row_upd && k <= nz - 2;
+            const bool h_upd = own && it >= 1;
+            cp_async_wait_group<1>();
+            stream_plane_barrier();
+            // own element of the previous stage: old H and H's x-slab
+            // auxiliaries; every lane of the quad reads before any refills it
+            Vf<1> hxm = fillv<1>(0.f), hym = hxm, hzm = hxm;
+            if (act) {
+                hxm.v[0] = stg(sp_, 0, r)[i];
+                hym.v[0] = stg(sp_, 1, r)[i];
+                hzm.v[0] = stg(sp_, 2, r)[i];
             }
-            const float *sp = a.src.n ? src_plane(a.src, k) : nullptr;
-            if (!CPML)
-                stream_e_quad<false, true, false, LOSSY, COH>(ex, ey, ez, hx, hy, hz, hxm, hym, hx_jm, hz_jm, hy_im0,
-                                                              hz_im0, b0, b1, b2, c0, c1, c2, xse, yze, ptab, a, i0,
-                                                              sp, ij0, nxy, dx, div);
-            else if (xw)
-                stream_e_quad<true, true, true, LOSSY, COH>(ex, ey, ez, hx, hy, hz, hxm, hym, hx_jm, hz_jm, hy_im0,
-                                                            hz_im0, b0, b1, b2, c0, c1, c2, xse, yze, ptab, a, i0, sp,
-                                                            ij0, nxy, dx, div);
-            else if (!yz_plane(k))
-                stream_e_quad<false, false, false, LOSSY, COH>(ex, ey, ez, hx, hy, hz, hxm, hym, hx_jm, hz_jm, hy_im0,
-                                                               hz_im0, b0, b1, b2, c0, c1, c2, xse, yze, ptab, a, i0,
-                                                               sp, ij0, nxy, dx, div);
-            else
-                stream_e_quad<false, false, true, LOSSY, COH>(ex, ey, ez, hx, hy, hz, hxm, hym, hx_jm, hz_jm, hy_im0,
-                                                              hz_im0, b0, b1, b2, c0, c1, c2, xse, yze, ptab, a, i0,
-                                                              sp, ij0, nxy, dx, div);
-        }
-        if (act) {
-            const int b = it & 1;
-            sts4(esp(b, 0, r) + i0, ex);
-            sts4(esp(b, 1, r) + i0, ey);
-            sts4(esp(b, 2, r) + i0, ez);
-        }
-        if (own && it < n) {
-            const long long g = ij0 + nxy * k;
-            stv<4>(a.f_out[0] + g, ex);
-            stv<4>(a.f_out[1] + g, ey);
-            stv<4>(a.f_out[2] + g, ez);
-            if (CPML && (xw || yz_plane(k))) stream_psi_store<0>(xse, yze, a, q, j, k, ij0, nxy, xw);
-        }
+            XPsi<1> xsh;
+            xsh.valid[0] = false; xsh.p0[0] = xsh.p1[0] = 0.f;
+            if (h_upd) stream_xpsi<1>(xsh, xrow(sp_, 2, r), xrow(sp_, 3, r), nx, L, i);
+            __syncwarp();
+            issue(it + 2, false);
 
-        // ---- H_new(k-1) of rows j0..j0+R-1: own old H and x-slab auxiliaries
-        //      from the previous stage, the new E of plane k-1 from the shared
-        //      array of iteration it-1 (own cells and neighbours), the new E of
-        //      plane k from registers
-        if (h_upd) {
-            const int km = k - 1;
-            const int b = (it - 1) & 1;
-            const Vf<4> exm = lds4(esp(b, 0, r) + i0), eym = lds4(esp(b, 1, r) + i0), ezm = lds4(esp(b, 2, r) + i0);
-            const Vf<4> ex_jp = lds4(esp(b, 0, r + 1) + i0), ez_jp = lds4(esp(b, 2, r + 1) + i0);
-            const float ey_ipw = q < QX - 1 ? esp(b, 1, r)[i0 + 4] : 0.f;
-            const float ez_ipw = q < QX - 1 ? esp(b, 2, r)[i0 + 4] : 0.f;
-            Vf<4> nhx = hxm, nhy = hym, nhz = hzm;
-            const float *sp = a.src.n ? src_plane(a.src, km) : nullptr;
-            if (!CPML)
-                stream_h_quad<false, true, false, COH>(nhx, nhy, nhz, ex, ey, exm, eym, ezm, ex_jp, ez_jp, ey_ipw,
-                                                       ez_ipw, xsh, yzh, ptab, a, i0, sp, ij0, nxy, dx, div, hb);
-            else if (xw)
-                stream_h_quad<true, true, true, COH>(nhx, nhy, nhz, ex, ey, exm, eym, ezm, ex_jp, ez_jp, ey_ipw,
-                                                     ez_ipw, xsh, yzh, ptab, a, i0, sp, ij0, nxy, dx, div, hb);
-            else if (!yz_plane(km))
-                stream_h_quad<false, false, false, COH>(nhx, nhy, nhz, ex, ey, exm, eym, ezm, ex_jp, ez_jp, ey_ipw,
-                                                        ez_ipw, xsh, yzh, ptab, a, i0, sp, ij0, nxy, dx, div, hb);
-            else
-                stream_h_quad<false, false, true, COH>(nhx, nhy, nhz, ex, ey, exm, eym, ezm, ex_jp, ez_jp, ey_ipw,
-                                                       ez_ipw, xsh, yzh, ptab, a, i0, sp, ij0, nxy, dx, div, hb);
-            const long long g = ij0 + nxy * km;
-            stv<4>(a.f_out[3] + g, nhx);
-            stv<4>(a.f_out[4] + g, nhy);
-            stv<4>(a.f_out[5] + g, nhz);
-            if (CPML && (xw || yz_plane(km))) stream_psi_store<2>(xsh, yzh, a, q, j, km, ij0, nxy, xw);
+            // ---- E_new(k) of this cell
+            Vf<1> ex = fillv<1>(0.f), ey = ex, ez = ex;
+            if (act) {
+                ex.v[0] = stg(s, 3, r)[i];
+                ey.v[0] = stg(s, 4, r)[i];
+                ez.v[0] = stg(s, 5, r)[i];
+            }
+            XPsi<1> xse;
+            xse.valid[0] = false; xse.p0[0] = xse.p1[0] = 0.f;
+            if (e_upd) {
+                stream_xpsi<1>(xse, xrow(s, 0, r), xrow(s, 1, r), nx, L, i);
+                Vf<1> hx, hy, hz, hx_jm, hz_jm, b0, b1, b2, c0 = fillv<1>(1.f), c1 = c0, c2 = c0;
+                hx.v[0] = stg(s, 0, r)[i];
+                hy.v[0] = stg(s, 1, r)[i];
+                hz.v[0] = stg(s, 2, r)[i];
+                hx_jm.v[0] = (r > 0 ? stg(s, 0, r - 1) : hlw(s, 0))[i];
+                hz_jm.v[0] = (r > 0 ? stg(s, 2, r - 1) : hlw(s, 1))[i];
+                const float hy_im0 = i > 0 ? stg(s, 1, r)[i - 1] : 0.f;
+                const float hz_im0 = i > 0 ? stg(s, 2, r)[i - 1] : 0.f;
+                b0.v[0] = stg(s, 6, r)[i];
+                b1.v[0] = stg(s, 7, r)[i];
+                b2.v[0] = stg(s, 8, r)[i];
+                if (LOSSY) {
+                    c0.v[0] = stg(s, 9, r)[i];
+                    c1.v[0] = stg(s, 10, r)[i];
+                    c2.v[0] = stg(s, 11, r)[i];
+                }
+                const float *sp = a.src.n ? src_plane(a.src, k) : nullptr;
+                stream_e_group<1, true, true, true, LOSSY, COH>(ex, ey, ez, hx, hy, hz, hxm, hym, hx_jm, hz_jm, hy_im0,
+                                                                hz_im0, b0, b1, b2, c0, c1, c2, xse, yze, ptab, a, i,
+                                                                sp, ij, nxy, dx, div);
+            }
+            if (act) {
+                const int b = it & 1;
+                esp(b, 0, r)[i] = ex.v[0];
+                esp(b, 1, r)[i] = ey.v[0];
+                esp(b, 2, r)[i] = ez.v[0];
+            }
+            if (own && it < n) {
+                const long long g = ij + nxy * k;
+                a.f_out[0][g] = ex.v[0];
+                a.f_out[1][g] = ey.v[0];
+                a.f_out[2][g] = ez.v[0];
+                stream_psi_store<1, 0, true>(xse, yze, a, i, j, k, ij, nxy);
+            }
+
+            // ---- H_new(k-1) of this cell (owned rows)
+            if (h_upd) {
+                const int km = k - 1;
+                const int b = (it - 1) & 1;
+                Vf<1> exm, eym, ezm, ex_jp, ez_jp;
+                exm.v[0] = esp(b, 0, r)[i];
+                eym.v[0] = esp(b, 1, r)[i];
+                ezm.v[0] = esp(b, 2, r)[i];
+                ex_jp.v[0] = esp(b, 0, r + 1)[i];
+                ez_jp.v[0] = esp(b, 2, r + 1)[i];
+                const float ey_ipw = i < nx - 1 ? esp(b, 1, r)[i + 1] : 0.f;
+                const float ez_ipw = i < nx - 1 ? esp(b, 2, r)[i + 1] : 0.f;
+                Vf<1> nhx = hxm, nhy = hym, nhz = hzm;
+                const float *sp = a.src.n ? src_plane(a.src, km) : nullptr;
+                stream_h_group<1, true, true, true, COH>(nhx, nhy, nhz, ex, ey, exm, eym, ezm, ex_jp, ez_jp, ey_ipw,
+                                                         ez_ipw, xsh, yzh, ptab, a, i, sp, ij, nxy, dx, div, hb);
+                const long long g = ij + nxy * km;
+                a.f_out[3][g] = nhx.v[0];
+                a.f_out[4][g] = nhy.v[0];
+                a.f_out[5][g] = nhz.v[0];
+                stream_psi_store<1, 2, true>(xsh, yzh, a, i, j, km, ij, nxy);
+            }
+            load_yz(it + 1);
         }
-        load_yz(it + 1);
+        cp_async_wait_group<0>();
     }
-    cp_async_wait_group<0>();
 }
 
 }  // namespace fdtd

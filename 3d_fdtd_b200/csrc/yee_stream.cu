@@ -71,16 +71,18 @@ static size_t stream_smem_floats(int nx, int ty, bool lossy, int L)
 }
 
 // split items 0..n-1 of cost c[] into at most `parts` contiguous runs of at
-// most `maxlen` items each, minimising the largest run cost (binary search on
-// that cost); returns the run starts (size = runs actually used) or empty
-static std::vector<int> split_runs(const std::vector<double> &c, int parts, int maxlen)
+// most `maxlen` items each, a run starting at every item t with brk[t] set
+// (brk may be empty), minimising the largest run cost (binary search on that
+// cost); returns the run starts (size = runs actually used) or empty
+static std::vector<int> split_runs(const std::vector<double> &c, int parts, int maxlen,
+                                   const std::vector<char> &brk = {})
 {
     const int n = (int)c.size();
     auto greedy = [&](double cap, std::vector<int> *starts) {
         int runs = 0, len = 0;
         double acc = 0;
         for (int t = 0; t < n; t++) {
-            if (len == 0 || acc + c[t] > cap || len >= maxlen) {
+            if (len == 0 || acc + c[t] > cap || len >= maxlen || (!brk.empty() && brk[t])) {
                 if (len > 0 || runs == 0) {
                     runs++;
                     if (starts) starts->push_back(t);
@@ -122,40 +124,70 @@ bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan 
                           stream_roles(nx, L, ty_max + 1).threads > kStreamMaxThreads))
         ty_max--;
     ty_max = std::min(ty_max, rows);
-    // bytes per cell of each row / plane (60 B, plus 32 B per CPML axis)
+    // Relative cost of a tile: (sum of its rows' costs + a band's fixed cost)
+    // x (sum of its planes' weights).  An interior row costs its 60 B a cell
+    // plus 2L x 32 B for its x-slab cells, a y-slab row 160 B a cell; a
+    // z-slab plane 1.27 times an interior one; and a band's plane costs 10
+    // interior rows more than its rows: a plane's pass is bound by the
+    // latency of its update chain about as much as by its bytes, so thin
+    // bands are hardly faster a plane.  Fitted to per-tile times on the 200 x
+    // 160 x 400 grid with and without a 12-cell CPML.
     std::vector<double> rc(rows), pc(planes);
+    std::vector<char> brk(rows, 0);
     for (int t = 0; t < rows; t++) {
         const int jj = 1 + t;
         const bool ys = L > 0 && (jj < L || jj >= ny - L);
-        rc[t] = (60.0 + (ys ? 32.0 : 0.0)) * nx + (L > 0 ? 64.0 * L : 0.0) + 44.0 * nx / std::max(1, ty_max);
+        rc[t] = (ys ? 160.0 : 60.0) * nx + 64.0 * L;
+        // a band is wholly inside or outside the y slabs: one y-slab row puts
+        // the whole band on the CPML path
+        brk[t] = L > 0 && (jj == L || jj == ny - L);
     }
     for (int t = 0; t < planes; t++) {
         const int kk = 1 + t;
-        const bool zs = L > 0 && (kk < L || kk >= nz - L);
-        pc[t] = 60.0 + (zs ? 32.0 : 0.0);
+        pc[t] = L > 0 && (kk < L || kk >= nz - L) ? 1.27 : 1.0;
     }
-    // band count: the smallest that keeps >= 95 % of the SMs busy with chunks
-    // of at least 8 planes (shorter chunks re-read their boundary planes too often)
-    const int nb_min = (rows + ty_max - 1) / ty_max;
+    const double band_fixed = 600.0 * nx;
+    // bands: as few as the row limit allows between the slab boundaries, of
+    // even size there (a band's plane time hardly shrinks with fewer rows, so
+    // a thin remainder band would be the slowest); then chunks of planes per
+    // band, handed out one at a time to the band whose tiles are the most
+    // expensive, up to `nsm` tiles, none shorter than 8 planes (shorter
+    // chunks re-read their boundary planes too often).  With fewer than one
+    // SM a band (a share of a multi-grid sweep) every band is one tile.
+    std::vector<int> bs;
+    for (int t0 = 0; t0 < rows;) {
+        int t1 = t0 + 1;
+        while (t1 < rows && !brk[t1]) t1++;
+        const int len = t1 - t0, parts = (len + ty_max - 1) / ty_max;
+        for (int p = 0; p < parts; p++) bs.push_back(t0 + (int)((long long)len * p / parts));
+        t0 = t1;
+    }
+    const int nbands = (int)bs.size();
     const int nc_max = std::max(1, planes / 8);
-    int best_nb = -1, best_nc = 0;
-    double best_use = -1;
-    for (int nb = nb_min; nb <= std::min(rows, 4 * nb_min); nb++) {
-        const int nc = std::min(nsm / nb, nc_max);
-        if (nc < 1) break;
-        const double use = (double)nb * nc / nsm;
-        if (use > best_use + 1e-9) { best_use = use; best_nb = nb; best_nc = nc; }
-        if (use >= 0.95) break;
+    std::vector<double> bcost(nbands, band_fixed);
+    std::vector<int> nchunk(nbands, 1);
+    for (int b = 0; b < nbands; b++) {
+        const int r0 = bs[b], r1 = b + 1 < nbands ? bs[b + 1] : rows;
+        for (int t = r0; t < r1; t++) bcost[b] += rc[t];
+        // a halo row in a y slab: its threads run the CPML updates, the
+        // slowest of each plane's pass
+        const int jh = 1 + r1;
+        if (L > 0 && jh >= ny - L && jh < ny - 1 && !(1 + r0 >= ny - L)) bcost[b] += 200.0 * nx;
     }
-    if (best_nb < 0) { best_nb = nb_min; best_nc = 1; }
-    const std::vector<int> bs = split_runs(rc, best_nb, ty_max);
-    const std::vector<int> cs = split_runs(pc, best_nc, planes);
-    if (bs.empty() || cs.empty()) return false;
+    for (int used = nbands; used < nsm; used++) {
+        int best = -1;
+        for (int b = 0; b < nbands; b++)
+            if (nchunk[b] < nc_max && (best < 0 || bcost[b] / nchunk[b] > bcost[best] / nchunk[best])) best = b;
+        if (best < 0) break;
+        nchunk[best]++;
+    }
     out->tiles.clear();
     out->ty = 0;
-    for (size_t b = 0; b < bs.size(); b++) {
-        const int r0 = bs[b], r1 = b + 1 < bs.size() ? bs[b + 1] : rows;
+    for (int b = 0; b < nbands; b++) {
+        const int r0 = bs[b], r1 = b + 1 < nbands ? bs[b + 1] : rows;
         out->ty = std::max(out->ty, r1 - r0);
+        const std::vector<int> cs = split_runs(pc, nchunk[b], planes);
+        if (cs.empty()) return false;
         for (size_t c = 0; c < cs.size(); c++) {
             const int p0 = cs[c], p1 = c + 1 < cs.size() ? cs[c + 1] : planes;
             out->tiles.push_back(StreamTile{1 + r0, r1 - r0, 1 + p0, 1 + p1});

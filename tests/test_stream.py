@@ -48,21 +48,24 @@ def plan(fd, nx, ny, nz, L, lossy, nsm):
     (20, 16, 24, 4, 0, 148),
     (8, 3, 3, 0, 0, 1),            # one interior cell row
     (512, 40, 50, 0, 0, 132),
+    (200, 160, 400, 12, 0, 18),    # one grid's share of an 8-grid sweep: more bands than tiles asked for
 ])
 def test_stream_plan_covers_interior_once(fd, nx, ny, nz, L, lossy, nsm):
     p = plan(fd, nx, ny, nz, L, lossy, nsm)
     assert p is not None
     tiles, ty, threads, smem = p
-    assert 1 <= len(tiles) <= nsm
-    # 12 warps x 168 registers fit an SM; x-slab quads (row ends) get warps of their own
+    bands = len({t[0] for t in tiles})
+    assert 1 <= len(tiles) <= max(nsm, bands)
+    # 16 warps x 128 registers fit an SM; the cells of the x-slab quads (row
+    # ends) get a thread each, in warps of their own
     qx = nx // 4
     if L:
         ql, qr = (L + 3) // 4, max((L + 3) // 4, min(qx, (nx - L) // 4))
         qi = qr - ql
-        want = ((ty + 1) * qi + 31) // 32 * 32 + (ty + 1) * (qx - qi)
+        want = ((ty + 1) * qi + 31) // 32 * 32 + (ty + 1) * 4 * (qx - qi)
     else:
         want = (ty + 1) * qx
-    assert threads % 32 == 0 and threads == (want + 31) // 32 * 32 and threads <= 384
+    assert threads % 32 == 0 and threads == (want + 31) // 32 * 32 and threads <= 512
     na = 12 if lossy else 9
     xw = (2 * L + 3) // 4 * 4   # staged x-slab auxiliaries per row, padded to 16 bytes
     ptab = 3 * 6 * 2 * L        # slab-cell profiles: 3 axes x 6 profiles x 2L cells

@@ -668,11 +668,12 @@ static bool fast32_path(const Grid *g)
 }
 
 // which kernel design the fast path uses: the one-pass streaming kernel where
-// the grid allows it (FDTD_YEE_STREAM, and opt-in until measured), the
-// plane-streaming TMA / cp.async kernel on request, else the flat pair
+// the grid allows it (FDTD_YEE_STREAM, and FDTD_YEE_AUTO: it moves each array
+// once a step and measured faster than the flat pair with and without CPML),
+// the plane-streaming TMA / cp.async kernel on request, else the flat pair
 static bool stream_path(const Grid *g)
 {
-    return fast32_path(g) && g->yee_variant == FDTD_YEE_STREAM &&
+    return fast32_path(g) && (g->yee_variant == FDTD_YEE_STREAM || g->yee_variant == FDTD_YEE_AUTO) &&
            stream_supported(g->nx, g->ny, g->nz, g->sig_e, g->boundary == FDTD_BOUNDARY_CPML ? g->L : 0);
 }
 

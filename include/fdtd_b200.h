@@ -221,15 +221,18 @@ enum fdtd_status {
 };
 enum fdtd_precision { FDTD_F64 = 0, FDTD_F32 = 1 };
 /* FP32 grids with mu = 1, no magnetic loss and a CPML or PEC boundary run one of
- * four kernel designs: flat (one thread per cell, separate E and H launches),
+ * five kernel designs: flat (one thread per cell, separate E and H launches),
  * flat4 (separate E and H launches, four x cells per thread with 16-byte
  * accesses; nx % 4 == 0), fused (one launch per step streaming z-planes through
  * shared memory) or wave (flat4's cell updates, but timefield3d_run executes
  * whole chunks of steps -- monitors and scheduled source included -- in one
  * persistent launch ordered as a wavefront in z, so a sweep's planes stay in
  * L2; runs with probes or bound taper stores, and single steps, use flat4).
- * AUTO picks flat4 where nx allows, else flat.  wave's fields are
- * bit-identical to flat4's. */
+ * stream (one launch per step: each thread block streams a band of rows
+ * through its planes, E and H of a plane in one pass, reading each array once
+ * and writing the other field set; nx % 4 == 0).  AUTO picks stream where the
+ * grid allows it, else flat4 where nx allows, else flat.  wave's fields are
+ * bit-identical to flat4's; stream's agree with flat4's to float rounding. */
 enum fdtd_yee_variant {
     FDTD_YEE_AUTO = 0, FDTD_YEE_FLAT = 1, FDTD_YEE_FUSED = 2, FDTD_YEE_FLAT4 = 3, FDTD_YEE_WAVE = 4,
     FDTD_YEE_STREAM = 5

@@ -395,7 +395,9 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
     achieved = bytes_step / (kms / 1e3) / 1e9
     peak, peak_kind = peaks()
     wave = args.yee_variant == "wave"
-    kernel_tag = "yee_wave_si_taper_200x160x400_fp32" if wave else "yee_step_si_taper_200x160x400_fp32"
+    stream_kernel = args.yee_variant in ("auto", "stream")
+    kernel_tag = ("yee_wave_si_taper_200x160x400_fp32" if wave else
+                  "yee_stream_si_taper_200x160x400_fp32" if stream_kernel else "yee_step_si_taper_200x160x400_fp32")
     traffic = read_traffic(kernel_tag)
     # end to end through the public API, host clock
     barrier()
@@ -452,7 +454,9 @@ def our_arm(args, rank: int, world: int, local_rank: int) -> None:
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                              "kernel": ("wavefront launch (E, H, CPML, source, monitor partials), per step"
-                                        if wave else "Yee step (E and H update kernels, CPML terms)"),
+                                        if wave else
+                                        "one-pass streaming Yee kernel (E, H, CPML terms, scheduled source), per step"
+                                        if stream_kernel else "Yee step (E and H update kernels, CPML terms)"),
                              "bytes_per_launch": bytes_step, "avg_launch_ms": kms,
                              "timed_launches": kcnt.value,
                              "timed_sample": (f"one wavefront launch in {KTIME_PERIOD}" if wave else

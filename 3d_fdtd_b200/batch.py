@@ -173,7 +173,7 @@ def autotune(fd, cand: dict, steps: int = 64) -> tuple[int, dict]:
     slot = Slot(fd)
     times = {}
     short = dict(cand, steps=steps)
-    for variant in (fd.YEE_FLAT4, fd.YEE_FLAT, fd.YEE_FUSED):
+    for variant in (fd.YEE_STREAM, fd.YEE_FLAT4, fd.YEE_FLAT, fd.YEE_FUSED):
         slot.prepare(short, variant)
         slot.start()
         slot.transmission()

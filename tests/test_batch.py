@@ -53,7 +53,7 @@ def test_sweep_equals_single_runs(fd, gpu, B):
 def test_autotune_times_each_design(fd, gpu, B):
     c = B.candidates(1, seed=2)[0]
     best, times = B.autotune(fd, c, steps=32)
-    assert set(times) == {fd.YEE_FLAT4, fd.YEE_FLAT, fd.YEE_FUSED}
+    assert set(times) == {fd.YEE_STREAM, fd.YEE_FLAT4, fd.YEE_FLAT, fd.YEE_FUSED}
     assert best == min(times, key=times.get) and all(v > 0 for v in times.values())
 
 

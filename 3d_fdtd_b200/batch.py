@@ -19,9 +19,9 @@ Runner: `slots` candidates are resident at a time, each with its own grid,
 CUDA stream and captured graphs; their runs are queued and overlap on the GPU
 while the host prepares the next candidate of a finished slot (grids are
 reused when the shape repeats).  Every candidate's result is the same, bit for
-bit, as running it alone.  An autotuner times the Yee kernel designs (flat4,
-flat, fused) on each grid shape with the in-graph kernel timers and keeps the
-fastest.  Across GPUs the candidates are split by replicas.Ranks (rank r runs
+bit, as running it alone.  An autotuner times the Yee kernel designs
+(streaming, flat4, flat, fused) on each grid shape with the in-graph kernel
+timers and keeps the fastest.  Across GPUs the candidates are split by replicas.Ranks (rank r runs
 r, r + N, ...) and the transmissions gathered to every rank.
 
     python -m 3d_fdtd_b200.batch [--candidates 64] [--slots 4]

@@ -1,7 +1,7 @@
 """Surrogate-assisted taper optimisation: a tensor-core MLP trained on
-simulations from the candidate sweep proposes design steps; every step is
-confirmed by an FDTD run, and the adjoint gradient takes over when the
-surrogate's prediction misses the simulation.
+simulations from the candidate runner proposes designs, every proposal is
+confirmed by an FDTD run, against an adjoint-only optimiser with the same
+budget of FDTD runs.
 
 Design: the spline taper of batch.py (20 control widths in [0.5, 3.0] um,
 natural cubic spline, sub-pixel fill) on one fixed grid of the candidate
@@ -10,17 +10,26 @@ transmission t(lambda) = O_out / O_in at the 11 monitor wavelengths
 1.50..1.60 um as (Re, Im) -> 22 network outputs; T = |t|^2.
 Objective: mean T over the 11 wavelengths.
 
-Surrogate step: ascend the predicted objective along the network's input
-gradient (normalised, fixed step in um, clipped to the width bounds);
-simulate the proposal; if |T_pred - T_fdtd| > 1e-2 discard the surrogate's
-direction for this step and take an adjoint step instead (forward + CW
-adjoint run as the reference driver does, 3d_fdtd.c:97-165, spline-weighted
-edge gradient of |O_out| at 1.55 um); add the simulated point to the training
-set and fine-tune; accept a step only if the simulated objective improves,
-else halve the step.  Baseline: the same loop with adjoint steps only, given
-the same number of FDTD runs.
+Both arms start from the best design of the training set and are timed by the
+host clock:
+- adjoint-only, the reference driver's method (3d_fdtd.c:97-187): a forward
+  run with the taper's edge store bound, the phase-reversed CW adjoint at
+  1.55 um, the spline-weighted edge gradient of |O_out|
+  (fdtd_spline_store_gradient), a step of fixed length along it; the forward
+  run at the proposal confirms the step and gives the next gradient, so a
+  step costs two runs; a step that does not improve is retried at half length.
+- surrogate: ascent of the predicted objective on the network from 64 starts
+  in a trust region around the current design (batched forward and input
+  gradient calls), the k best distinct proposals simulated concurrently on k
+  slots of the candidate runner, the simulated points added to the training
+  set and the network fine-tuned; the region grows after an improvement and
+  shrinks after a miss.
+Reported: best objective against FDTD runs and wall time per arm, the time
+each arm takes to reach the adjoint arm's final best, the validation error of
+t against the training-set size, and the data-generation time (the fixed cost
+the surrogate pays once per design family).
 
-    python -m 3d_fdtd_b200.surrogate_opt [--train 1024] [--iters 12]
+    python -m 3d_fdtd_b200.surrogate_opt [--train 1024] [--budget 32] [--k 4]
 """
 from __future__ import annotations
 
@@ -29,6 +38,7 @@ import ctypes as C
 import importlib
 import json
 import math
+import os
 import time
 
 import numpy as np
@@ -53,9 +63,10 @@ def random_widths(seed: int) -> np.ndarray:
 
 
 def simulate(fd, widths_list, nz: int, steps: int, slots: int = 4):
-    """FDTD of every design (concurrent); returns complex t [n, 11]."""
+    """FDTD of every design (concurrent, default kernel design); returns
+    complex t [n, 11] and the runner's record."""
     cands = [design(w, i, nz, steps) for i, w in enumerate(widths_list)]
-    r = B.sweep(fd, cands, slots=slots, variant=fd.YEE_FLAT4)
+    r = B.sweep(fd, cands, slots=max(1, min(slots, len(cands))), variant=fd.YEE_AUTO)
     return np.array([r["amplitudes"][i] for i in range(len(cands))]), r
 
 
@@ -96,19 +107,22 @@ class Net:
         return dx[:n]
 
     def train(self, x: np.ndarray, y: np.ndarray, epochs: int, batch: int = 128, lr: float = 1e-3,
-              seed: int = 0) -> float:
+              lr_end: float | None = None, seed: int = 0) -> float:
+        """Adam over shuffled minibatches; with lr_end the rate follows a
+        cosine from lr to lr_end over the epochs."""
         rng = np.random.default_rng(seed)
         n = len(x)
         bs = min(batch, n // 8 * 8)
         loss = C.c_double()
         last = float("nan")
-        for _ in range(epochs):
+        for ep in range(epochs):
+            rate = lr if lr_end is None else lr_end + 0.5 * (lr - lr_end) * (1 + math.cos(math.pi * ep / epochs))
             order = rng.permutation(n)
             for s in range(0, n - bs + 1, bs):
                 idx = order[s:s + bs]
                 xb, yb = np.ascontiguousarray(x[idx], np.float32), np.ascontiguousarray(y[idx], np.float32)
                 self.fd.call("fdtd_mlp_train_step", self.h, xb.ctypes.data_as(FP), yb.ctypes.data_as(FP), bs,
-                             C.c_float(lr), C.byref(loss))
+                             C.c_float(rate), C.byref(loss))
                 last = loss.value
         return last
 
@@ -121,13 +135,18 @@ def mean_T_of_y(y: np.ndarray) -> np.ndarray:
     return (y[..., :NLAM] ** 2 + y[..., NLAM:] ** 2).mean(axis=-1)
 
 
-def adjoint_gradient(fd, widths: np.ndarray, nz: int, steps: int) -> np.ndarray:
-    """Spline-weighted adjoint gradient of |O_out(1.55 um)| with respect to
-    the widths (direction; the reference's formula omits a global constant)."""
+def mean_T(t: np.ndarray) -> float:
+    return float(np.mean(np.abs(t) ** 2))
+
+
+def adjoint_gradient(fd, widths: np.ndarray, nz: int, steps: int):
+    """(gradient, t): the spline-weighted adjoint gradient of |O_out(1.55 um)|
+    with respect to the widths (a direction: the reference's formula omits a
+    global constant), and the forward run's complex t(lambda)."""
     s = B.SPEC
     cand = design(widths, 0, nz, steps)
     slot = B.Slot(fd)
-    slot.prepare(cand, fd.YEE_FLAT4)
+    slot.prepare(cand, fd.YEE_AUTO)
     t = slot.grid.t
     b, top = s["core_y"]
     z0, z1 = s["margin"], nz - s["margin"]
@@ -138,6 +157,7 @@ def adjoint_gradient(fd, widths: np.ndarray, nz: int, steps: int) -> np.ndarray:
     try:
         fd.call("fdtd_spline_store_bind", store, t, 0, 0, 1)
         slot.start()
+        amp = slot.amplitudes()
         n = len(slot.omega)
         out = (fd.Complex * n)()
         fd.call("timefield3d_read_overlap_monitor", t, slot.mon_out, out)
@@ -161,62 +181,115 @@ def adjoint_gradient(fd, widths: np.ndarray, nz: int, steps: int) -> np.ndarray:
     finally:
         fd.lib.fdtd_spline_store_free(store)
         slot.close()
-    return grad
+    return grad, amp
 
 
-def optimise(fd, w0: np.ndarray, nz: int, steps: int, budget: int, step_um: float = 0.15, net: Net | None = None,
-             data: tuple | None = None, finetune_epochs: int = 20, log=None) -> dict:
-    """Ascend mean T from w0 within `budget` FDTD runs; surrogate steps when a
-    network is given, adjoint steps otherwise (and as the fallback)."""
+def optimise_adjoint(fd, w0: np.ndarray, nz: int, steps: int, budget: int, step_um: float = 0.15,
+                     log=None) -> dict:
+    """Adjoint-only ascent from w0 within `budget` FDTD runs (2 per step)."""
+    clock = time.perf_counter()
     w = np.asarray(w0, float).copy()
-    t0 = simulate(fd, [w], nz, steps, slots=1)[0][0]
-    best = float(np.mean(np.abs(t0) ** 2))
-    runs = 1
-    hist = [dict(run=runs, T=best, kind="start")]
-    X, Y = data if data is not None else (None, None)
-    fallbacks = 0
-    while runs < budget:
-        kind = "adjoint"
-        proposal = None
-        if net is not None:
-            x = norm_x(w)[None]
-            y = net.predict(x)
-            dy = np.concatenate([2 * y[:, :NLAM], 2 * y[:, NLAM:]], axis=1) / NLAM
-            g = net.input_gradient(x, dy.astype(np.float32))[0].astype(np.float64) / 1.25
-            if np.abs(g).max() > 0:
-                proposal = np.clip(w + step_um * g / np.abs(g).max(), W_LO, W_HI)
-                t_p = simulate(fd, [proposal], nz, steps, slots=1)[0][0]
-                runs += 1
-                T_fd = float(np.mean(np.abs(t_p) ** 2))
-                T_pred = float(mean_T_of_y(net.predict(norm_x(proposal)[None]))[0])
-                X = np.concatenate([X, norm_x(proposal)[None]])
-                Y = np.concatenate([Y, to_y(t_p[None])])
-                net.train(X, Y, finetune_epochs, batch=min(128, len(X) // 8 * 8), seed=runs)
-                kind = "surrogate"
-                if abs(T_pred - T_fd) > 1e-2:
-                    fallbacks += 1
-                    proposal = None
-                    kind = "surrogate miss -> adjoint"
-        if proposal is None:
-            if runs + 3 > budget:     # an adjoint step costs forward + adjoint + confirmation
-                break
-            g = adjoint_gradient(fd, w, nz, steps)
-            runs += 2
-            proposal = np.clip(w + step_um * g / max(np.abs(g).max(), 1e-30), W_LO, W_HI)
-            t_p = simulate(fd, [proposal], nz, steps, slots=1)[0][0]
-            runs += 1
-            T_fd = float(np.mean(np.abs(t_p) ** 2))
-            if X is not None:
-                X = np.concatenate([X, norm_x(proposal)[None]])
-                Y = np.concatenate([Y, to_y(t_p[None])])
-        if T_fd > best:
-            w, best = proposal, T_fd
+    g, t = adjoint_gradient(fd, w, nz, steps)
+    runs, best = 2, mean_T(t)
+    hist = [dict(run=runs, T=best, best=best, seconds=time.perf_counter() - clock, kind="start")]
+    while runs + 2 <= budget:
+        proposal = np.clip(w + step_um * g / max(np.abs(g).max(), 1e-30), W_LO, W_HI)
+        g_p, t_p = adjoint_gradient(fd, proposal, nz, steps)
+        runs += 2
+        T_p = mean_T(t_p)
+        if T_p > best:
+            w, best, g = proposal, T_p, g_p
         else:
             step_um *= 0.5
-        hist.append(dict(run=runs, T=T_fd, best=best, kind=kind, step=step_um))
+        hist.append(dict(run=runs, T=T_p, best=best, seconds=time.perf_counter() - clock, kind="adjoint",
+                         step=step_um))
         if log:
             log(hist[-1])
-    return dict(widths=w.tolist(), best=best, runs=runs, fallbacks=fallbacks, history=hist)
+    return dict(widths=w.tolist(), best=best, runs=runs, seconds=time.perf_counter() - clock, history=hist)
+
+
+def surrogate_proposals(net: Net, w: np.ndarray, radius: float, k: int, rng, starts: int = 64,
+                        substeps: int = 20) -> np.ndarray:
+    """Up to k distinct designs (apart by more than radius/10 in some width)
+    of highest predicted mean T, found by ascending the network's prediction
+    from `starts` points of the box |x - w| <= radius (per width, within the
+    bounds); the first start is w itself."""
+    lo, hi = np.maximum(w - radius, W_LO), np.minimum(w + radius, W_HI)
+    x = np.clip(w + rng.uniform(-radius, radius, (starts, NCTRL)), lo, hi)
+    x[0] = w
+    step = radius / substeps
+    for _ in range(substeps):
+        y = net.predict(norm_x(x))
+        dy = np.concatenate([2 * y[:, :NLAM], 2 * y[:, NLAM:]], axis=1) / NLAM
+        g = net.input_gradient(norm_x(x), dy.astype(np.float32)).astype(np.float64)
+        g /= np.maximum(np.abs(g).max(axis=1, keepdims=True), 1e-30)
+        x = np.clip(x + step * g, lo, hi)
+    pred = mean_T_of_y(net.predict(norm_x(x)))
+    chosen = []
+    for i in np.argsort(-pred):
+        if all(np.abs(x[i] - x[c]).max() > radius / 10 for c in chosen):
+            chosen.append(i)
+        if len(chosen) == k:
+            break
+    return x[chosen]
+
+
+def optimise_surrogate(fd, net: Net, data: tuple, w0: np.ndarray, T0: float, nz: int, steps: int, budget: int,
+                       k: int = 4, radius: float = 0.3, finetune_epochs: int = 20, seed: int = 0, log=None) -> dict:
+    """Surrogate-proposal ascent from w0 (mean T T0, already simulated: a
+    training design) within `budget` FDTD runs, k concurrent runs a round."""
+    clock = time.perf_counter()
+    rng = np.random.default_rng(seed)
+    X, Y = data
+    w, best, runs = np.asarray(w0, float).copy(), float(T0), 0
+    hist = [dict(run=0, T=best, best=best, seconds=0.0, kind="start")]
+    while runs + k <= budget:
+        props = surrogate_proposals(net, w, radius, k, rng)
+        pred = mean_T_of_y(net.predict(norm_x(props)))
+        t_p, _ = simulate(fd, list(props), nz, steps, slots=len(props))
+        runs += len(props)
+        T_p = np.mean(np.abs(t_p) ** 2, axis=1)
+        X = np.concatenate([X, norm_x(props)])
+        Y = np.concatenate([Y, to_y(t_p)])
+        net.train(X, Y, finetune_epochs, batch=min(128, len(X) // 8 * 8), lr=3e-4, seed=runs)
+        i = int(np.argmax(T_p))
+        if T_p[i] > best:
+            w, best = props[i].copy(), float(T_p[i])
+            radius = min(1.5 * radius, 0.6)
+        else:
+            radius *= 0.5
+        hist.append(dict(run=runs, T=float(T_p[i]), pred=float(pred[i]), best=best, radius=radius,
+                         seconds=time.perf_counter() - clock, kind="surrogate"))
+        if log:
+            log(hist[-1])
+    return dict(widths=w.tolist(), best=best, runs=runs, seconds=time.perf_counter() - clock, history=hist)
+
+
+def time_to(result: dict, target: float):
+    """(seconds, FDTD runs) at which an arm's best first reached `target`, or None."""
+    for h in result["history"]:
+        if h["best"] >= target - 1e-12:
+            return h["seconds"], h["run"]
+    return None
+
+
+def training_data(fd, n: int, nz: int, steps: int, cache: str | None):
+    """n seeded designs (seeds 1000..) and their simulated t, from the cache
+    file when it holds the same problem."""
+    widths = np.array([random_widths(1000 + i) for i in range(n)])
+    if cache and os.path.exists(cache):
+        z = np.load(cache)
+        if int(z["nz"]) == nz and int(z["steps"]) == steps and len(z["t"]) >= n and \
+                np.array_equal(z["widths"][:n], widths):
+            return widths, z["t"][:n], dict(seconds=float(z["seconds"]) * n / len(z["t"]), cached=True,
+                                            mcell_updates_per_s=float(z["rate"]))
+    t0 = time.perf_counter()
+    t, sweep = simulate(fd, list(widths), nz, steps)
+    seconds = time.perf_counter() - t0
+    rate = sweep["cell_steps"] / sweep["seconds"] / 1e6
+    if cache:
+        np.savez(cache, widths=widths, t=t, nz=nz, steps=steps, seconds=seconds, rate=rate)
+    return widths, t, dict(seconds=seconds, cached=False, mcell_updates_per_s=rate)
 
 
 def main():
@@ -224,37 +297,55 @@ def main():
     ap.add_argument("--train", type=int, default=1024)
     ap.add_argument("--nz", type=int, default=128)
     ap.add_argument("--steps", type=int, default=4451)
-    ap.add_argument("--epochs", type=int, default=300)
-    ap.add_argument("--budget", type=int, default=30)
+    ap.add_argument("--epochs", type=int, default=1000)
+    ap.add_argument("--budget", type=int, default=32)
+    ap.add_argument("--k", type=int, default=4, help="surrogate proposals simulated together per round")
+    ap.add_argument("--sizes", default="128,256,512", help="smaller training sets for the accuracy curve")
+    ap.add_argument("--data", default=None, help="npz cache of the training simulations")
     args = ap.parse_args()
     fd = importlib.import_module("3d_fdtd_b200")
-    t0 = time.perf_counter()
-    n_all = args.train + max(8, args.train // 8)
-    widths = [random_widths(1000 + i) for i in range(n_all)]
-    t, sweep = simulate(fd, widths, args.nz, args.steps)
-    t_data = time.perf_counter() - t0
-    X, Y = norm_x(np.array(widths)), to_y(t)
+    n_val = max(8, args.train // 8)
+    widths, t, gen = training_data(fd, args.train + n_val, args.nz, args.steps, args.data)
+    X, Y = norm_x(widths), to_y(t)
     Xtr, Ytr, Xva, Yva = X[:args.train], Y[:args.train], X[args.train:], Y[args.train:]
-    net = Net(fd)
-    t1 = time.perf_counter()
-    loss = net.train(Xtr, Ytr, args.epochs)
-    t_train = time.perf_counter() - t1
-    pred = net.predict(Xva)
-    T_va, T_pred = mean_T_of_y(Yva), mean_T_of_y(pred)
+
+    def fit(n):
+        net = Net(fd)
+        t1 = time.perf_counter()
+        loss = net.train(Xtr[:n], Ytr[:n], args.epochs, lr=1e-3, lr_end=1e-5)
+        pred = net.predict(Xva)
+        return net, dict(samples=n, final_loss=loss, seconds=time.perf_counter() - t1,
+                         val_rmse_t=float(np.sqrt(np.mean((pred - Yva) ** 2))),
+                         val_mae_meanT=float(np.mean(np.abs(mean_T_of_y(pred) - mean_T_of_y(Yva)))))
+
+    by_size = []
+    for n in sorted({int(v) for v in args.sizes.split(",") if v} - {args.train}):
+        if 8 <= n < args.train:
+            net_n, rec = fit(n)
+            net_n.close()
+            by_size.append(rec)
+    net, rec = fit(args.train)
+    by_size.append(rec)
     start = int(np.argmax(mean_T_of_y(Ytr)))
-    w0 = np.array(widths[start])
-    sur = optimise(fd, w0, args.nz, args.steps, args.budget, net=net, data=(Xtr.copy(), Ytr.copy()))
-    adj = optimise(fd, w0, args.nz, args.steps, args.budget)
+    w0, T0 = widths[start], float(mean_T_of_y(Ytr)[start])
+    adj = optimise_adjoint(fd, w0, args.nz, args.steps, args.budget)
+    sur = optimise_surrogate(fd, net, (Xtr.copy(), Ytr.copy()), w0, T0, args.nz, args.steps, args.budget, k=args.k)
     net.close()
+    target = adj["best"]
+    reach_s, reach_a = time_to(sur, target), time_to(adj, target)
     print(json.dumps(dict(
         problem=dict(grid=[256, 128, args.nz], steps=args.steps, controls=NCTRL, wavelengths=NLAM),
-        data=dict(runs=n_all, seconds=t_data, mcell_updates_per_s=sweep["cell_steps"] / sweep["seconds"] / 1e6),
-        training=dict(samples=args.train, epochs=args.epochs, final_loss=loss, seconds=t_train,
-                      val_rmse_t=float(np.sqrt(np.mean((pred - Yva) ** 2))),
-                      val_mae_meanT=float(np.mean(np.abs(T_pred - T_va)))),
-        start=dict(index=start, meanT=float(mean_T_of_y(Ytr)[start])),
-        surrogate=dict(best_meanT=sur["best"], fdtd_runs=sur["runs"], fallbacks=sur["fallbacks"]),
-        adjoint_only=dict(best_meanT=adj["best"], fdtd_runs=adj["runs"]),
+        data=dict(runs=len(widths), **gen),
+        training=dict(epochs=args.epochs, by_size=by_size),
+        start=dict(index=start, meanT=T0),
+        adjoint_only=dict(best_meanT=adj["best"], fdtd_runs=adj["runs"], seconds=adj["seconds"],
+                          curve=[(h["run"], round(h["seconds"], 3), h["best"]) for h in adj["history"]]),
+        surrogate=dict(best_meanT=sur["best"], fdtd_runs=sur["runs"], seconds=sur["seconds"], k=args.k,
+                       curve=[(h["run"], round(h["seconds"], 3), h["best"]) for h in sur["history"]]),
+        time_to_adjoint_best=dict(target_meanT=target,
+                                  surrogate=None if reach_s is None else dict(seconds=reach_s[0], runs=reach_s[1]),
+                                  adjoint_only=None if reach_a is None else dict(seconds=reach_a[0], runs=reach_a[1]),
+                                  speedup=None if reach_s is None or reach_s[0] <= 0 else reach_a[0] / reach_s[0]),
         target_meanT=0.95)), flush=True)
 
 

@@ -10,8 +10,8 @@ transmission t(lambda) = O_out / O_in at the 11 monitor wavelengths
 1.50..1.60 um as (Re, Im) -> 22 network outputs; T = |t|^2.
 Objective: mean T over the 11 wavelengths.
 
-Both arms start from the best design of the training set and are timed by the
-host clock:
+The arms start from the best design of the training set, share the budget of
+FDTD runs and are timed by the host clock:
 - adjoint-only, the reference driver's method (3d_fdtd.c:97-187): a forward
   run with the taper's edge store bound, the phase-reversed CW adjoint at
   1.55 um, the spline-weighted edge gradient of |O_out|
@@ -24,6 +24,9 @@ host clock:
   slots of the candidate runner, the simulated points added to the training
   set and the network fine-tuned; the region grows after an improvement and
   shrinks after a miss.
+- adjoint steps sized by the surrogate: the adjoint arm's directions, with the
+  step length along each chosen by the network's prediction (the network
+  fine-tuned on every simulated point).
 Reported: best objective against FDTD runs and wall time per arm, the time
 each arm takes to reach the adjoint arm's final best, the validation error of
 t against the training-set size, and the data-generation time (the fixed cost
@@ -105,6 +108,16 @@ class Net:
         self.fd.call("fdtd_mlp_input_gradient", self.h, xp.ctypes.data_as(FP), dyp.ctypes.data_as(FP), len(xp),
                      dx.ctypes.data_as(FP))
         return dx[:n]
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.fd.lib.fdtd_mlp_param_count(self.h), np.float32)
+        self.fd.call("fdtd_mlp_get_params", self.h, p.ctypes.data_as(FP))
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        """Weights from get_params (the optimiser state restarts)."""
+        p = np.ascontiguousarray(p, np.float32)
+        self.fd.call("fdtd_mlp_set_params", self.h, p.ctypes.data_as(FP))
 
     def train(self, x: np.ndarray, y: np.ndarray, epochs: int, batch: int = 128, lr: float = 1e-3,
               lr_end: float | None = None, seed: int = 0) -> float:
@@ -203,6 +216,44 @@ def optimise_adjoint(fd, w0: np.ndarray, nz: int, steps: int, budget: int, step_
             step_um *= 0.5
         hist.append(dict(run=runs, T=T_p, best=best, seconds=time.perf_counter() - clock, kind="adjoint",
                          step=step_um))
+        if log:
+            log(hist[-1])
+    return dict(widths=w.tolist(), best=best, runs=runs, seconds=time.perf_counter() - clock, history=hist)
+
+
+STEP_LENGTHS = (0.025, 0.05, 0.1, 0.15, 0.2, 0.3, 0.45, 0.6)
+
+
+def optimise_hybrid(fd, net: Net, data: tuple, w0: np.ndarray, nz: int, steps: int, budget: int,
+                    finetune_epochs: int = 20, log=None) -> dict:
+    """Adjoint directions, step lengths chosen by the network: along each
+    adjoint direction the network predicts mean T at STEP_LENGTHS (times a
+    trust factor, halved after a step that does not improve) and the best is
+    simulated; the simulated point joins the training set.  2 runs a step, as
+    the adjoint-only arm."""
+    clock = time.perf_counter()
+    X, Y = data
+    w = np.asarray(w0, float).copy()
+    g, t = adjoint_gradient(fd, w, nz, steps)
+    runs, best, trust = 2, mean_T(t), 1.0
+    hist = [dict(run=runs, T=best, best=best, seconds=time.perf_counter() - clock, kind="start")]
+    while runs + 2 <= budget:
+        d = g / max(np.abs(g).max(), 1e-30)
+        cands = np.array([np.clip(w + trust * s * d, W_LO, W_HI) for s in STEP_LENGTHS])
+        pred = mean_T_of_y(net.predict(norm_x(cands)))
+        proposal = cands[int(np.argmax(pred))]
+        g_p, t_p = adjoint_gradient(fd, proposal, nz, steps)
+        runs += 2
+        T_p = mean_T(t_p)
+        X = np.concatenate([X, norm_x(proposal)[None]])
+        Y = np.concatenate([Y, to_y(t_p[None])])
+        net.train(X, Y, finetune_epochs, batch=min(128, len(X) // 8 * 8), lr=3e-4, seed=runs)
+        if T_p > best:
+            w, best, g = proposal, T_p, g_p
+        else:
+            trust *= 0.5
+        hist.append(dict(run=runs, T=T_p, pred=float(pred.max()), best=best, seconds=time.perf_counter() - clock,
+                         kind="hybrid", trust=trust))
         if log:
             log(hist[-1])
     return dict(widths=w.tolist(), best=best, runs=runs, seconds=time.perf_counter() - clock, history=hist)
@@ -328,24 +379,31 @@ def main():
     by_size.append(rec)
     start = int(np.argmax(mean_T_of_y(Ytr)))
     w0, T0 = widths[start], float(mean_T_of_y(Ytr)[start])
+    params = net.get_params()
     adj = optimise_adjoint(fd, w0, args.nz, args.steps, args.budget)
     sur = optimise_surrogate(fd, net, (Xtr.copy(), Ytr.copy()), w0, T0, args.nz, args.steps, args.budget, k=args.k)
+    net.set_params(params)
+    hyb = optimise_hybrid(fd, net, (Xtr.copy(), Ytr.copy()), w0, args.nz, args.steps, args.budget)
     net.close()
     target = adj["best"]
-    reach_s, reach_a = time_to(sur, target), time_to(adj, target)
+
+    def arm(r, **extra):
+        return dict(best_meanT=r["best"], fdtd_runs=r["runs"], seconds=r["seconds"], **extra,
+                    curve=[(h["run"], round(h["seconds"], 3), h["best"]) for h in r["history"]])
+
+    def reach(r):
+        x = time_to(r, target)
+        return None if x is None else dict(seconds=x[0], runs=x[1])
     print(json.dumps(dict(
         problem=dict(grid=[256, 128, args.nz], steps=args.steps, controls=NCTRL, wavelengths=NLAM),
         data=dict(runs=len(widths), **gen),
         training=dict(epochs=args.epochs, by_size=by_size),
         start=dict(index=start, meanT=T0),
-        adjoint_only=dict(best_meanT=adj["best"], fdtd_runs=adj["runs"], seconds=adj["seconds"],
-                          curve=[(h["run"], round(h["seconds"], 3), h["best"]) for h in adj["history"]]),
-        surrogate=dict(best_meanT=sur["best"], fdtd_runs=sur["runs"], seconds=sur["seconds"], k=args.k,
-                       curve=[(h["run"], round(h["seconds"], 3), h["best"]) for h in sur["history"]]),
-        time_to_adjoint_best=dict(target_meanT=target,
-                                  surrogate=None if reach_s is None else dict(seconds=reach_s[0], runs=reach_s[1]),
-                                  adjoint_only=None if reach_a is None else dict(seconds=reach_a[0], runs=reach_a[1]),
-                                  speedup=None if reach_s is None or reach_s[0] <= 0 else reach_a[0] / reach_s[0]),
+        adjoint_only=arm(adj),
+        surrogate=arm(sur, k=args.k),
+        adjoint_steps_sized_by_surrogate=arm(hyb),
+        time_to_adjoint_best=dict(target_meanT=target, adjoint_only=reach(adj), surrogate=reach(sur),
+                                  adjoint_steps_sized_by_surrogate=reach(hyb)),
         target_meanT=0.95)), flush=True)
 
 

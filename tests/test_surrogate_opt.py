@@ -41,6 +41,11 @@ def test_optimisation_loop_small(fd, gpu):
         check_arm(O, sur, 6)
         adj = O.optimise_adjoint(fd, w0, nz, steps, budget=6)
         check_arm(O, adj, 6)
+        p = net.get_params()
+        net.set_params(p)
+        assert np.array_equal(net.get_params(), p)
+        hyb = O.optimise_hybrid(fd, net, (X.copy(), Y.copy()), w0, nz, steps, budget=6, finetune_epochs=5)
+        check_arm(O, hyb, 6)
         assert O.time_to(adj, adj["best"]) is not None
     finally:
         net.close()

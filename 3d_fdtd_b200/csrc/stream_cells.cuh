@@ -55,11 +55,26 @@ __device__ __forceinline__ void sts2(float *p, const Vf<2> &x) { *reinterpret_ca
 template <int W> struct XPsi {
     bool valid[W];
     float p0[W], p1[W];
+    float b[W], c[W], k[W];     // the x profiles (b, a, 1/kappa) of a single x-slab cell (W = 1)
 };
 template <int W> struct YZPsi {
     int sj, sk;
     Vf<W> pxy, pzy, pxz, pyz;   // as YZSlab: (x,y) (z,y) (x,z) (y,z) for E, alike for H
+    float py[3], pz[3];         // y and z profiles (b, a, 1/kappa) of a single x-slab cell (W = 1)
 };
+
+// x-slab auxiliaries of one x-slab cell from a staged row pair, with the
+// cell's slab-local index and x profiles kept in registers for the tile
+__device__ __forceinline__ void stream_xpsi_cell(XPsi<1> &xs, const float *row0, const float *row1, int si, bool valid,
+                                                 const float (&prof)[3])
+{
+    xs.valid[0] = valid;
+    xs.p0[0] = valid ? row0[si] : 0.f;
+    xs.p1[0] = valid ? row1[si] : 0.f;
+    xs.b[0] = prof[0];
+    xs.c[0] = prof[1];
+    xs.k[0] = prof[2];
+}
 
 // x-slab auxiliaries of the group at x = i0.. from a staged row pair (row0,
 // row1: the two auxiliaries of this field for the cell row)
@@ -96,9 +111,11 @@ __device__ __forceinline__ void stream_profile_table(float *pt, const StreamArgs
 
 // COH: plain (coherent) loads, for launches in which other blocks wrote the
 // auxiliaries (the multi-step sweep); else the read-only path
+// (a single x-slab cell, W = 1, also takes its y and z profiles from the
+// tile's table `pt` here, an iteration before they are used)
 template <int W, int A0, bool COH>
 __device__ __forceinline__ void stream_yzpsi_load(YZPsi<W> &s, const StreamArgs &a, int i0, int j, int k,
-                                                  long long ij0, long long nxy)
+                                                  long long ij0, long long nxy, const float *pt = nullptr)
 {
     const int nx = a.nx, L = a.L;
     s.sj = slab_local(j, a.ny, L);
@@ -108,11 +125,21 @@ __device__ __forceinline__ void stream_yzpsi_load(YZPsi<W> &s, const StreamArgs 
         const long long sy = (long long)i0 + (long long)nx * (s.sj + 2LL * L * k);
         s.pxy = ldf<W, COH>(a.psi_in[1][A0] + sy);
         s.pzy = ldf<W, COH>(a.psi_in[1][A0 + 1] + sy);
+        if constexpr (W == 1) {
+            const float *py = pt + (6 + 3 * (A0 / 2)) * 2 * L + s.sj;
+#pragma unroll
+            for (int w = 0; w < 3; w++) s.py[w] = py[w * 2 * L];
+        }
     }
     if (s.sk >= 0) {
         const long long sz = ij0 + nxy * s.sk;
         s.pxz = ldf<W, COH>(a.psi_in[2][A0] + sz);
         s.pyz = ldf<W, COH>(a.psi_in[2][A0 + 1] + sz);
+        if constexpr (W == 1) {
+            const float *pz = pt + (12 + 3 * (A0 / 2)) * 2 * L + s.sk;
+#pragma unroll
+            for (int w = 0; w < 3; w++) s.pz[w] = pz[w * 2 * L];
+        }
     }
 }
 
@@ -167,9 +194,13 @@ __device__ __forceinline__ Curl3 stream_cpml_curl(XPsi<W> &xs, YZPsi<W> &s, cons
     const int PL = 2 * L;
     float pyx = 0.f, pzx = 0.f, kx = 1.f;
     if (X && xs.valid[e]) {
-        const float *px = pt + pw * PL + slab_local(i, nx, L);
-        const float b = px[0], c = px[PL];
-        kx = px[2 * PL];
+        float b, c;
+        if constexpr (W == 1) {
+            b = xs.b[e]; c = xs.c[e]; kx = xs.k[e];
+        } else {
+            const float *px = pt + pw * PL + slab_local(i, nx, L);
+            b = px[0]; c = px[PL]; kx = px[2 * PL];
+        }
         pyx = b * xs.p0[e] + c * (d_zx * div);
         pzx = b * xs.p1[e] + c * (d_yx * div);
         xs.p0[e] = pyx;
@@ -177,18 +208,26 @@ __device__ __forceinline__ Curl3 stream_cpml_curl(XPsi<W> &xs, YZPsi<W> &s, cons
     }
     float vxy = 0.f, vzy = 0.f, vxz = 0.f, vyz = 0.f, ky = 1.f, kz = 1.f;
     if (s.sj >= 0) {
-        const float *py = pt + (6 + pw) * PL + s.sj;
-        const float by = py[0], ay = py[PL];
-        ky = py[2 * PL];
+        float by, ay;
+        if constexpr (W == 1) {
+            by = s.py[0]; ay = s.py[1]; ky = s.py[2];
+        } else {
+            const float *py = pt + (6 + pw) * PL + s.sj;
+            by = py[0]; ay = py[PL]; ky = py[2 * PL];
+        }
         vxy = by * s.pxy.v[e] + ay * (d_zy * div);
         vzy = by * s.pzy.v[e] + ay * (d_xy * div);
         s.pxy.v[e] = vxy;
         s.pzy.v[e] = vzy;
     }
     if (s.sk >= 0) {
-        const float *pz = pt + (12 + pw) * PL + s.sk;
-        const float bz = pz[0], az = pz[PL];
-        kz = pz[2 * PL];
+        float bz, az;
+        if constexpr (W == 1) {
+            bz = s.pz[0]; az = s.pz[1]; kz = s.pz[2];
+        } else {
+            const float *pz = pt + (12 + pw) * PL + s.sk;
+            bz = pz[0]; az = pz[PL]; kz = pz[2 * PL];
+        }
         vxz = bz * s.pxz.v[e] + az * (d_yz * div);
         vyz = bz * s.pyz.v[e] + az * (d_xz * div);
         s.pxz.v[e] = vxz;
@@ -566,6 +605,16 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
         auto yz_plane = [&](int k) { return y_row || z_plane(k); };
         const bool whole = xquad_whole(i0, nx, L);
         const int si = slab_local(i, nx, L);
+        const bool xvalid = si >= 0 && i >= 1 && i <= nx - 2;   // x terms updated at this cell
+        // the cell's x profiles (b, a, 1/kappa of E, then of H), for the tile
+        float pxe[3] = {0.f, 0.f, 1.f}, pxh[3] = {0.f, 0.f, 1.f};
+        if (xvalid) {
+#pragma unroll
+            for (int w = 0; w < 3; w++) {
+                pxe[w] = __ldg(a.prof[w][0] + i);
+                pxh[w] = __ldg(a.prof[3 + w][0] + i);
+            }
+        }
         // source array of staged array `arr` (selects, no branches: the lanes of
         // a warp take different arrays)
         auto src_of = [&](int arr) -> const float * {
@@ -609,8 +658,8 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
             if (it > n) return;
             const int k = tl.k0 + it;
             if (!yz_plane(k) && !yz_plane(k - 1)) return;
-            if (act && row_upd && k <= nz - 2) stream_yzpsi_load<1, 0, COH>(yze, a, i, j, k, ij, nxy);
-            if (own && it >= 1) stream_yzpsi_load<1, 2, COH>(yzh, a, i, j, k - 1, ij, nxy);
+            if (act && row_upd && k <= nz - 2) stream_yzpsi_load<1, 0, COH>(yze, a, i, j, k, ij, nxy, ptab);
+            if (own && it >= 1) stream_yzpsi_load<1, 2, COH>(yzh, a, i, j, k - 1, ij, nxy, ptab);
         };
         load_yz(0);
 
@@ -630,8 +679,7 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
                 hzm.v[0] = stg(sp_, 2, r)[i];
             }
             XPsi<1> xsh;
-            xsh.valid[0] = false; xsh.p0[0] = xsh.p1[0] = 0.f;
-            if (h_upd) stream_xpsi<1>(xsh, xrow(sp_, 2, r), xrow(sp_, 3, r), nx, L, i);
+            stream_xpsi_cell(xsh, xrow(sp_, 2, r), xrow(sp_, 3, r), si, h_upd && xvalid, pxh);
             __syncwarp();
             issue(it + 2, false);
 
@@ -643,9 +691,8 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
                 ez.v[0] = stg(s, 5, r)[i];
             }
             XPsi<1> xse;
-            xse.valid[0] = false; xse.p0[0] = xse.p1[0] = 0.f;
+            stream_xpsi_cell(xse, xrow(s, 0, r), xrow(s, 1, r), si, e_upd && xvalid, pxe);
             if (e_upd) {
-                stream_xpsi<1>(xse, xrow(s, 0, r), xrow(s, 1, r), nx, L, i);
                 Vf<1> hx, hy, hz, hx_jm, hz_jm, b0, b1, b2, c0 = fillv<1>(1.f), c1 = c0, c2 = c0;
                 hx.v[0] = stg(s, 0, r)[i];
                 hy.v[0] = stg(s, 1, r)[i];

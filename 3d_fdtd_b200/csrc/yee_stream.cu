@@ -126,27 +126,27 @@ bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan 
     ty_max = std::min(ty_max, rows);
     // Relative cost of a tile: (sum of its rows' costs + a band's fixed cost)
     // x (sum of its planes' weights).  An interior row costs its 60 B a cell
-    // plus 2L x 32 B for its x-slab cells, a y-slab row 160 B a cell; a
-    // z-slab plane 1.27 times an interior one; and a band's plane costs 10
-    // interior rows more than its rows: a plane's pass is bound by the
-    // latency of its update chain about as much as by its bytes, so thin
-    // bands are hardly faster a plane.  Fitted to per-tile times on the 200 x
-    // 160 x 400 grid with and without a 12-cell CPML.
+    // plus 2L x 32 B for its x-slab cells, a y-slab row 126 B a cell; a
+    // z-slab plane 1.67 times an interior one; and a band's plane costs about
+    // 3.6 interior rows more than its rows: a plane's pass is bound by the
+    // latency of its update chain as well as by its bytes, so thin bands are
+    // slower a row.  Fitted to per-tile times (%globaltimer per block) on the
+    // 200 x 160 x 400 grid with a 12-cell CPML.
     std::vector<double> rc(rows), pc(planes);
     std::vector<char> brk(rows, 0);
     for (int t = 0; t < rows; t++) {
         const int jj = 1 + t;
         const bool ys = L > 0 && (jj < L || jj >= ny - L);
-        rc[t] = (ys ? 160.0 : 60.0) * nx + 64.0 * L;
+        rc[t] = (ys ? 126.0 : 60.0) * nx + 64.0 * L;
         // a band is wholly inside or outside the y slabs: one y-slab row puts
         // the whole band on the CPML path
         brk[t] = L > 0 && (jj == L || jj == ny - L);
     }
     for (int t = 0; t < planes; t++) {
         const int kk = 1 + t;
-        pc[t] = L > 0 && (kk < L || kk >= nz - L) ? 1.27 : 1.0;
+        pc[t] = L > 0 && (kk < L || kk >= nz - L) ? 1.67 : 1.0;
     }
-    const double band_fixed = 600.0 * nx;
+    const double band_fixed = 218.0 * nx;
     // bands: as few as the row limit allows between the slab boundaries, of
     // even size there (a band's plane time hardly shrinks with fewer rows, so
     // a thin remainder band would be the slowest); then chunks of planes per
@@ -172,7 +172,7 @@ bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan 
         // a halo row in a y slab: its threads run the CPML updates, the
         // slowest of each plane's pass
         const int jh = 1 + r1;
-        if (L > 0 && jh >= ny - L && jh < ny - 1 && !(1 + r0 >= ny - L)) bcost[b] += 200.0 * nx;
+        if (L > 0 && jh >= ny - L && jh < ny - 1 && !(1 + r0 >= ny - L)) bcost[b] += 190.0 * nx;
     }
     for (int used = nbands; used < nsm; used++) {
         int best = -1;

@@ -93,8 +93,8 @@ __device__ __forceinline__ void stream_xpsi(XPsi<W> &xs, const float *row0, cons
 
 // Shared profile table of a tile: [axis x, y, z][profile 0..5][2L slab-local
 // cells] (profiles 0..2: b, a, 1/kappa of E; 3..5 of H; slab-local index as
-// slab_local), filled by the whole block.  The caller's first barrier orders
-// the fill before any read.
+// slab_local), filled by the whole block; the caller puts a block barrier
+// between the fill and any read.
 __device__ __forceinline__ void stream_profile_table(float *pt, const StreamArgs &a)
 {
     const int L = a.L, PL = 2 * L;
@@ -411,7 +411,10 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
     float *hlow = xps + (size_t)S * 4 * TP * XW;     // [S][2][nx]: Hx, Hz of row j0-1
     float *es = hlow + (size_t)S * 2 * nx;           // [2][3][TP][nx]: new E of the last two planes
     float *ptab = es + (size_t)2 * 3 * TP * nx;      // CPML profiles of the slab cells (stream_profile_table)
-    if (CPML) stream_profile_table(ptab, a);
+    if (CPML) {
+        stream_profile_table(ptab, a);
+        __syncthreads();   // x-slab cells read the table before the first plane's barrier
+    }
     // shared-memory offsets fit 32 bits (the whole allocation is < 64K floats)
     auto stg = [&](int s, int arr, int row) -> float * { return stage + ((s * NA + arr) * TP + row) * nx; };
     auto xrow = [&](int s, int arr, int row) -> float * { return xps + ((s * 4 + arr) * TP + row) * XW; };

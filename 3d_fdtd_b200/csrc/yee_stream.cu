@@ -124,29 +124,30 @@ bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan 
                           stream_roles(nx, L, ty_max + 1).threads > kStreamMaxThreads))
         ty_max--;
     ty_max = std::min(ty_max, rows);
-    // Relative cost of a tile: (sum of its rows' costs + a band's fixed cost)
-    // x (sum of its planes' weights).  An interior row costs its 60 B a cell
-    // plus 2L x 32 B for its x-slab cells, a y-slab row 126 B a cell; a
-    // z-slab plane 1.67 times an interior one; and a band's plane costs about
-    // 3.6 interior rows more than its rows: a plane's pass is bound by the
-    // latency of its update chain as well as by its bytes, so thin bands are
-    // slower a row.  Fitted to per-tile times (%globaltimer per block) on the
-    // 200 x 160 x 400 grid with a 12-cell CPML.
-    std::vector<double> rc(rows), pc(planes);
+    // Cost of a tile: its band's time a plane x (sum of its planes' weights).
+    // A plane's pass is bound by the latency of the update chain as well as
+    // by the bytes, so a band's plane time is a fixed part plus a part a row:
+    // 0.90 + 0.22 R us for interior bands and 1.88 + 0.32 R us for bands in
+    // a y slab (their updates carry the CPML recursion on every cell), with
+    // 0.8 us more when a band's halo row lies in a y slab (those threads run
+    // the CPML update; the band cuts avoid that), and the row part scaled by
+    // nx / 200; a z-slab plane
+    // weighs 1.67.  Fitted to per-tile times (%globaltimer per block) on the
+    // 200 x 160 x 400 grid with a 12-cell CPML; only the ratios matter.
+    std::vector<double> pc(planes);
     std::vector<char> brk(rows, 0);
     for (int t = 0; t < rows; t++) {
         const int jj = 1 + t;
-        const bool ys = L > 0 && (jj < L || jj >= ny - L);
-        rc[t] = (ys ? 126.0 : 60.0) * nx + 64.0 * L;
-        // a band is wholly inside or outside the y slabs: one y-slab row puts
-        // the whole band on the CPML path
-        brk[t] = L > 0 && (jj == L || jj == ny - L);
+        // bands split where the y slabs begin, so that interior bands hold no
+        // y-slab row; above the interior the cut is one row early, so that no
+        // interior band's halo row (the row above its last) lies in the slab
+        brk[t] = L > 0 && (jj == L || jj == ny - L - 1);
     }
     for (int t = 0; t < planes; t++) {
         const int kk = 1 + t;
         pc[t] = L > 0 && (kk < L || kk >= nz - L) ? 1.67 : 1.0;
     }
-    const double band_fixed = 218.0 * nx;
+    const double sx = nx / 200.0;
     // bands: as few as the row limit allows between the slab boundaries, of
     // even size there (a band's plane time hardly shrinks with fewer rows, so
     // a thin remainder band would be the slowest); then chunks of planes per
@@ -164,15 +165,14 @@ bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan 
     }
     const int nbands = (int)bs.size();
     const int nc_max = std::max(1, planes / 8);
-    std::vector<double> bcost(nbands, band_fixed);
+    std::vector<double> bcost(nbands);
     std::vector<int> nchunk(nbands, 1);
     for (int b = 0; b < nbands; b++) {
         const int r0 = bs[b], r1 = b + 1 < nbands ? bs[b + 1] : rows;
-        for (int t = r0; t < r1; t++) bcost[b] += rc[t];
-        // a halo row in a y slab: its threads run the CPML updates, the
-        // slowest of each plane's pass
-        const int jh = 1 + r1;
-        if (L > 0 && jh >= ny - L && jh < ny - 1 && !(1 + r0 >= ny - L)) bcost[b] += 190.0 * nx;
+        const int j0 = 1 + r0, jh = 1 + r1;   // first row, halo row
+        const bool yb = L > 0 && (j0 < L || jh - 1 >= ny - L);
+        bcost[b] = yb ? 1.88 + 0.32 * sx * (r1 - r0) : 0.90 + 0.22 * sx * (r1 - r0);
+        if (!yb && L > 0 && jh >= ny - L && jh < ny - 1) bcost[b] += 0.8;
     }
     for (int used = nbands; used < nsm; used++) {
         int best = -1;

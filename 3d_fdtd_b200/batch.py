@@ -252,7 +252,7 @@ def _sweep_call(fd, slots, nsteps, steps_per_launch, band_rows, tiles_per_sm):
 
 
 def autotune_tiles(fd, cands: list[dict], steps: int = 128, steps_per_launch: int = 64,
-                   shapes=((0, 1.0), (0, 2.0), (4, 1.0), (3, 1.0), (3, 2.0))) -> tuple[tuple[int, float], dict]:
+                   shapes=((0, 2.0), (0, 4.0), (0, 8.0), (4, 4.0), (3, 4.0))) -> tuple[tuple[int, float], dict]:
     """Tile shape of the persistent sweep: for each (band rows cap, tiles per
     SM) the sweep of these candidates runs `steps` steps after a warm-up, timed
     on the host around a synchronised call; the fastest shape is returned."""

@@ -1331,10 +1331,11 @@ bool run_sweep(const std::vector<Grid *> &gs, double dt, const std::vector<int> 
                int ty_cap, double tiles_per_sm)
 {
     const int ng = (int)gs.size();
-    if (ng <= 0 || (int)nsteps.size() != ng || steps_per_launch < 1 || steps_per_launch > 4096 || ty_cap < 0 ||
-        !(tiles_per_sm > 0) || tiles_per_sm > 16) {
-        set_error(FDTD_ERR_ARG, "sweep: no grids, or steps_per_launch not in [1, 4096], ty_cap < 0, or tiles_per_sm "
-                                "not in (0, 16]");
+    if (ng <= 0 || ng > kSweepMaxGrids || (int)nsteps.size() != ng || steps_per_launch < 1 ||
+        steps_per_launch > 4096 || ty_cap < 0 || !(tiles_per_sm > 0) || tiles_per_sm > 16) {
+        set_error(FDTD_ERR_ARG, "sweep: grids not in [1, %d], or steps_per_launch not in [1, 4096], ty_cap < 0, or "
+                                "tiles_per_sm not in (0, 16]",
+                  kSweepMaxGrids);
         return false;
     }
     int nsm = 0;
@@ -1458,8 +1459,16 @@ bool run_sweep(const std::vector<Grid *> &gs, double dt, const std::vector<int> 
         launches.push_back(std::move(row));
         lsteps.push_back(lmax);
     }
+    // every grid's tiles, most expensive first (the blocks take them in this order)
+    std::vector<std::pair<double, int2>> order;
+    for (int i = 0; i < ng; i++)
+        for (int t = 0; t < (int)plans[i].tiles.size(); t++)
+            order.push_back({stream_tile_cost(gs[i]->nx, gs[i]->ny, gs[i]->nz, L0, plans[i].tiles[t]), make_int2(i, t)});
+    std::stable_sort(order.begin(), order.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+    std::vector<int2> items;
+    for (auto &o : order) items.push_back(o.second);
     if (!launches.empty() &&
-        !sweep_launch(launches, lsteps, L0 > 0, g0->sig_e, threads, smem, 1000000000ull))
+        !sweep_launch(launches, lsteps, items, L0 > 0, g0->sig_e, threads, smem, 1000000000ull))
         return false;
     // the grids' own streams continue after the sweep
     CK(cudaEventRecord(sweep_event(), sst));

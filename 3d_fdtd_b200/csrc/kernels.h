@@ -217,6 +217,8 @@ int stream_supported(int nx, int ny, int nz, bool lossy, int L);
 // tiles for a grid over nsm blocks (one per SM); ty_cap > 0 caps the rows of a
 // band (the autotuner's tile-shape knob); false when the grid cannot use the kernel
 bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan *out, int ty_cap = 0);
+// the plan's cost estimate of one tile (relative)
+double stream_tile_cost(int nx, int ny, int nz, int L, const StreamTile &t);
 // allow `smem` bytes of dynamic shared memory for every instantiation and check
 // that blocks of `threads` threads can launch (host, not stream-ordered)
 bool stream_configure(size_t smem, int threads);
@@ -224,6 +226,7 @@ void launch_yee_stream(const StreamArgs &a, const StreamPlan &p, cudaStream_t st
 
 // yee_sweep.cu: many grids advanced together by persistent launches of S
 // steps (see the file's header); one entry per grid per launch
+constexpr int kSweepMaxGrids = 48;   // grids of one sweep call (their tile arguments sit in constant memory)
 struct SweepGrid {
     StreamArgs args[2];          // input set p (output 1 - p); args[p].tiles = this grid's sweep tiles
     int ntiles;
@@ -244,6 +247,9 @@ struct SweepGrid {
 struct SweepArgs {
     const SweepGrid *grids;
     int ngrids, steps;           // steps: the most of any grid
+    const int2 *items;           // every grid's tiles as (grid, tile), most expensive first
+    int nitems;
+    unsigned *next;              // per step of the launch: next item to hand out (zero at launch start)
     unsigned *bar;               // barrier arrivals, zero when the launch starts
     int *err;                    // set when a barrier wait gives up
     unsigned long long wait_ns;
@@ -255,8 +261,9 @@ cudaEvent_t sweep_event();
 int *sweep_err();
 StreamTile **sweep_tiles(size_t bytes);     // grown device buffers owned by the sweep
 double2 **sweep_partials(size_t bytes);
-bool sweep_launch(const std::vector<std::vector<SweepGrid>> &launches, const std::vector<int> &steps, bool cpml,
-                  bool lossy, int threads, size_t smem, unsigned long long wait_ns);
+bool sweep_launch(const std::vector<std::vector<SweepGrid>> &launches, const std::vector<int> &steps,
+                  const std::vector<int2> &items, bool cpml, bool lossy, int threads, size_t smem,
+                  unsigned long long wait_ns);
 void launch_sweep_err_to_grid(const int *sweep, int *grid, cudaStream_t st);
 bool sweep_barrier_selftest(unsigned long long limit_ns, int *timed_out);
 

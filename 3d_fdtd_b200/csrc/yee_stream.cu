@@ -114,6 +114,27 @@ int stream_supported(int nx, int ny, int nz, bool lossy, int L)
     return stream_smem_floats(nx, 1, lossy, L) * sizeof(float) <= kStreamSmemBudget;
 }
 
+// Time of a band's pass over one plane (us; only ratios matter): rows
+// [j0, j0 + rows) with its halo row j0 + rows.  See stream_plan.
+static double band_plane_cost(int nx, int ny, int L, int j0, int rows)
+{
+    const double sx = nx / 200.0;
+    const int jh = j0 + rows;
+    const bool yb = L > 0 && (j0 < L || jh - 1 >= ny - L);
+    double c = yb ? 1.88 + 0.32 * sx * rows : 0.90 + 0.22 * sx * rows;
+    if (!yb && L > 0 && jh >= ny - L && jh < ny - 1) c += 0.8;
+    return c;
+}
+
+static double plane_weight(int nz, int L, int k) { return L > 0 && (k < L || k >= nz - L) ? 1.67 : 1.0; }
+
+double stream_tile_cost(int nx, int ny, int nz, int L, const StreamTile &t)
+{
+    double w = 0;
+    for (int k = t.k0; k < t.k1; k++) w += plane_weight(nz, L, k);
+    return band_plane_cost(nx, ny, L, t.j0, t.rows) * w;
+}
+
 bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan *out, int ty_cap)
 {
     if (!stream_supported(nx, ny, nz, lossy, L) || nsm <= 0 || ty_cap < 0) return false;
@@ -143,11 +164,7 @@ bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan 
         // interior band's halo row (the row above its last) lies in the slab
         brk[t] = L > 0 && (jj == L || jj == ny - L - 1);
     }
-    for (int t = 0; t < planes; t++) {
-        const int kk = 1 + t;
-        pc[t] = L > 0 && (kk < L || kk >= nz - L) ? 1.67 : 1.0;
-    }
-    const double sx = nx / 200.0;
+    for (int t = 0; t < planes; t++) pc[t] = plane_weight(nz, L, 1 + t);
     // bands: as few as the row limit allows between the slab boundaries, of
     // even size there (a band's plane time hardly shrinks with fewer rows, so
     // a thin remainder band would be the slowest); then chunks of planes per
@@ -169,10 +186,7 @@ bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan 
     std::vector<int> nchunk(nbands, 1);
     for (int b = 0; b < nbands; b++) {
         const int r0 = bs[b], r1 = b + 1 < nbands ? bs[b + 1] : rows;
-        const int j0 = 1 + r0, jh = 1 + r1;   // first row, halo row
-        const bool yb = L > 0 && (j0 < L || jh - 1 >= ny - L);
-        bcost[b] = yb ? 1.88 + 0.32 * sx * (r1 - r0) : 0.90 + 0.22 * sx * (r1 - r0);
-        if (!yb && L > 0 && jh >= ny - L && jh < ny - 1) bcost[b] += 0.8;
+        bcost[b] = band_plane_cost(nx, ny, L, 1 + r0, r1 - r0);
     }
     for (int used = nbands; used < nsm; used++) {
         int best = -1;

@@ -7,7 +7,11 @@
 // SM, all co-resident), each candidate for at most its own remaining steps.
 // Per step, three phases separated by grid barriers where needed:
 //   A  the one-pass FP32 Yee update (yee_stream.cu) of every candidate still
-//      running: its (band, chunk) tiles, dealt round robin over the blocks;
+//      running: all candidates' (band, chunk) tiles in one list ordered by
+//      estimated cost, longest first, each block taking the next tile from a
+//      per-step counter when it finishes one (tiles of candidates of every
+//      length, so dealing them out statically left the blocks' phase times
+//      up to 2x apart);
 //   -- barrier --
 //   B  each candidate's step tail: the overlap partials of its monitors (one
 //      warp per partial, the same partial as the per-step tail's 256-thread
@@ -30,6 +34,8 @@
 #include "stream_cells.cuh"
 #include "plane_ops.cuh"
 #include "engine.h"
+
+#include <algorithm>
 
 #define CK_RET(call)                               \
     do {                                           \
@@ -95,27 +101,44 @@ __device__ bool sweep_barrier(const SweepArgs &a, unsigned k, int *abort_s)
     return *abort_s == 0;
 }
 
+// The tile arguments of every grid of a sweep (grid g, input set p at 2g + p)
+// in constant memory, as a kernel's parameters are for the per-step launch:
+// read from a global-memory copy the tile held its dozens of pointers in
+// registers and spilled, and its planes took twice as long.
+__constant__ StreamArgs c_sweep_args[2 * kSweepMaxGrids];
+static_assert(sizeof(c_sweep_args) <= 60 * 1024, "sweep tile arguments must fit constant memory");
+
+// One tile, out of line, so that the persistent loop's state and the phase
+// B/C code do not share the tile's registers.
+template <bool CPML, bool LOSSY>
+__device__ __forceinline__ void sweep_tile(int idx, int t, float *sm)
+{
+    const StreamArgs &sa = c_sweep_args[idx];
+    stream_tile<CPML, LOSSY, true>(sa, sa.tiles[t], sm);
+}
+
 template <bool CPML, bool LOSSY>
 __global__ void __launch_bounds__(kStreamMaxThreads, 1) k_sweep(SweepArgs a)
 {
     extern __shared__ __align__(16) float sm[];
-    __shared__ int abort_s;
+    __shared__ int abort_s, item_s;
     const int G = gridDim.x, warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gw = blockIdx.x * warps + warp, nw = G * warps;
     unsigned nbar = 0;
     for (int s = 0; s < a.steps; s++) {
-        // ---- A: Yee tiles of the running grids, round robin over the blocks
-        int item = 0;
-        for (int g = 0; g < a.ngrids; g++) {
-            const SweepGrid &sg = a.grids[g];
+        // ---- A: Yee tiles of the running grids, handed out one at a time
+        //      from a list ordered by cost (longest first), so the blocks
+        //      finish the step together whatever the grids' lengths
+        for (;;) {
+            __syncthreads();   // the block's previous tile no longer reads shared memory; item_s is free
+            if (threadIdx.x == 0) item_s = (int)atomicAdd(a.next + s, 1u);
+            __syncthreads();
+            const int idx = item_s;
+            if (idx >= a.nitems) break;
+            const int2 it = a.items[idx];
+            const SweepGrid &sg = a.grids[it.x];
             if (s >= sg.steps) continue;
-            const int first = (blockIdx.x - item % G + G) % G;   // this block's first tile of the grid
-            for (int t = first; t < sg.ntiles; t += G) {
-                __syncthreads();   // the block's previous tile no longer reads shared memory
-                const StreamArgs &sa = sg.args[(sg.p0 + s) & 1];
-                stream_tile<CPML, LOSSY, true>(sa, sa.tiles[t], sm);
-            }
-            item += sg.ntiles;
+            sweep_tile<CPML, LOSSY>(2 * it.x + ((sg.p0 + s) & 1), it.y, sm);
         }
         if (!sweep_barrier(a, ++nbar, &abort_s)) return;
         // ---- B: overlap partials of step s, scheduled source of step s+1
@@ -199,6 +222,9 @@ struct SweepContext {
     cudaStream_t st = nullptr;
     int dev = -1, nsm = 0;
     unsigned *d_bar = nullptr;
+    unsigned *d_next = nullptr;   // per step of a launch, the next tile item (kSweepMaxSteps)
+    int2 *d_items = nullptr;
+    size_t items_cap = 0;
     int *d_err = nullptr;
     SweepGrid *d_grids = nullptr;
     size_t grids_cap = 0;
@@ -244,6 +270,7 @@ bool sweep_setup(int *nsm_out)
         CK_RET(cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking));
         CK_RET(cudaEventCreateWithFlags(&c.ev, cudaEventDisableTiming));
         CK_RET(cudaMalloc(&c.d_bar, sizeof(unsigned)));
+        CK_RET(cudaMalloc(&c.d_next, 4096 * sizeof(unsigned)));   // steps_per_launch <= 4096
         CK_RET(cudaMalloc(&c.d_err, sizeof(int)));
         CK_RET(cudaMemset(c.d_err, 0, sizeof(int)));
     }
@@ -254,15 +281,26 @@ bool sweep_setup(int *nsm_out)
 // Runs the launches described by `launches` (each a list of SweepGrid, one per
 // grid) on the sweep stream as one captured graph.  Tile tables and partial
 // buffers are the caller's (already uploaded to `tiles`/`partials`).
-bool sweep_launch(const std::vector<std::vector<SweepGrid>> &launches, const std::vector<int> &steps, bool cpml,
-                  bool lossy, int threads, size_t smem, unsigned long long wait_ns)
+bool sweep_launch(const std::vector<std::vector<SweepGrid>> &launches, const std::vector<int> &steps,
+                  const std::vector<int2> &items, bool cpml, bool lossy, int threads, size_t smem,
+                  unsigned long long wait_ns)
 {
     SweepContext &c = ctx();
     const int ng = launches.empty() ? 0 : (int)launches[0].size();
     const size_t per = (size_t)ng;
     std::vector<SweepGrid> flat;
     for (auto &l : launches) flat.insert(flat.end(), l.begin(), l.end());
-    CK_RET(cudaStreamSynchronize(c.st));
+    if (ng > kSweepMaxGrids) return false;
+    CK_RET(cudaStreamSynchronize(c.st));   // no sweep of this context reads the constant arguments now
+    {
+        std::vector<StreamArgs> args;
+        for (int g = 0; g < ng; g++)
+            for (int p = 0; p < 2; p++) args.push_back(launches[0][g].args[p]);
+        if (!args.empty())
+            CK_RET(cudaMemcpyToSymbolAsync(c_sweep_args, args.data(), args.size() * sizeof(StreamArgs), 0,
+                                           cudaMemcpyHostToDevice, c.st));
+        CK_RET(cudaStreamSynchronize(c.st));
+    }
     CK_RET(cudaMemsetAsync(c.d_err, 0, sizeof(int), c.st));
     if (c.exec) {
         cudaGraphExecDestroy(c.exec);
@@ -270,6 +308,9 @@ bool sweep_launch(const std::vector<std::vector<SweepGrid>> &launches, const std
     }
     if (!grow(&c.d_grids, c.grids_cap, flat.size() * sizeof(SweepGrid))) return false;
     CK_RET(cudaMemcpyAsync(c.d_grids, flat.data(), flat.size() * sizeof(SweepGrid), cudaMemcpyHostToDevice, c.st));
+    if (!grow(&c.d_items, c.items_cap, std::max<size_t>(items.size(), 1) * sizeof(int2))) return false;
+    if (!items.empty())
+        CK_RET(cudaMemcpyAsync(c.d_items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice, c.st));
     const void *fn = cpml ? (lossy ? sweep_kernel<true, true>() : sweep_kernel<true, false>())
                           : (lossy ? sweep_kernel<false, true>() : sweep_kernel<false, false>());
     CK_RET(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -288,11 +329,15 @@ bool sweep_launch(const std::vector<std::vector<SweepGrid>> &launches, const std
         a.grids = c.d_grids + l * per;
         a.ngrids = ng;
         a.steps = steps[l];
+        a.items = c.d_items;
+        a.nitems = (int)items.size();
+        a.next = c.d_next;
         a.bar = c.d_bar;
         a.err = c.d_err;
         a.wait_ns = wait_ns;
         a.arrivals = (unsigned)c.nsm;
-        ok = cudaMemsetAsync(c.d_bar, 0, sizeof(unsigned), c.st) == cudaSuccess;
+        ok = cudaMemsetAsync(c.d_bar, 0, sizeof(unsigned), c.st) == cudaSuccess &&
+             cudaMemsetAsync(c.d_next, 0, (size_t)std::max(1, steps[l]) * sizeof(unsigned), c.st) == cudaSuccess;
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3((unsigned)c.nsm);
         cfg.blockDim = dim3((unsigned)threads);

@@ -1315,8 +1315,9 @@ int fdtd_sweep_run(const timefield3d *grids, int ngrids, double delta_t, const i
                    int band_rows, double tiles_per_sm)
 {
     LOCK;
-    if (!grids || !nsteps || ngrids <= 0 || !(delta_t > 0) || !std::isfinite(delta_t)) {
-        set_error(FDTD_ERR_ARG, "fdtd_sweep_run: grids, nsteps, ngrids > 0 and a positive delta_t are required");
+    if (!grids || !nsteps || ngrids <= 0 || ngrids > kSweepMaxGrids || !(delta_t > 0) || !std::isfinite(delta_t)) {
+        set_error(FDTD_ERR_ARG, "fdtd_sweep_run: grids, nsteps, ngrids in [1, %d] and a positive delta_t are required",
+                  kSweepMaxGrids);
         return FDTD_ERR_ARG;
     }
     std::vector<Grid *> gs;

@@ -290,7 +290,10 @@ bool sweep_launch(const std::vector<std::vector<SweepGrid>> &launches, const std
     const size_t per = (size_t)ng;
     std::vector<SweepGrid> flat;
     for (auto &l : launches) flat.insert(flat.end(), l.begin(), l.end());
-    if (ng > kSweepMaxGrids) return false;
+    if (ng > kSweepMaxGrids) {
+        set_error(FDTD_ERR_ARG, "sweep: more than %d grids", kSweepMaxGrids);
+        return false;
+    }
     CK_RET(cudaStreamSynchronize(c.st));   // no sweep of this context reads the constant arguments now
     {
         std::vector<StreamArgs> args;

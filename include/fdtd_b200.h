@@ -475,7 +475,8 @@ int fdtd_wait_selftest(double limit_seconds, double *elapsed_seconds);
  * stores) and ends exactly as timefield3d_run would leave it.  Tile shape:
  * band_rows caps the rows of a band (0: as many as shared memory allows);
  * tiles_per_sm sets how many tiles per SM the grids are cut into per step
- * (in (0, 16]).  A grid barrier that waits more than 1 s ends the launch;
+ * (in (0, 16]; the blocks take the tiles of all grids from one queue, longest
+ * first, so finer tiles balance better).  At most 48 grids per call.  A grid barrier that waits more than 1 s ends the launch;
  * the grids then report FDTD_ERR_TIMEOUT at their next synchronising call. */
 int fdtd_sweep_run(const timefield3d *grids, int ngrids, double delta_t, const int *nsteps, int steps_per_launch,
                    int band_rows, double tiles_per_sm);

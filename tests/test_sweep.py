@@ -95,5 +95,10 @@ def test_sweep_rejects_bad_arguments(fd):
     # refused on the host before any device work
     assert fd.lib.fdtd_sweep_run(None, 0, 0.01, None, 64, 0, 1.0) == fd.FDTD_ERR_ARG
     fd.lib.fdtd_clear_error()
+    # at most 48 grids a call (their tile arguments sit in constant memory)
+    grids = (fd.Timefield3d * 49)()
+    steps = (C.c_int * 49)(*([1] * 49))
+    assert fd.lib.fdtd_sweep_run(grids, 49, 0.01, steps, 64, 0, 1.0) == fd.FDTD_ERR_ARG
+    fd.lib.fdtd_clear_error()
     assert fd.lib.fdtd_sweep_barrier_selftest(-1.0) in (fd.FDTD_ERR_ARG, fd.FDTD_ERR_NO_DEVICE)
     fd.lib.fdtd_clear_error()

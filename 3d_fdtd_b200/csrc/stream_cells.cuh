@@ -8,6 +8,9 @@
 namespace fdtd {
 
 constexpr int kStreamStages = 3;
+// cell index within one array of a streaming grid: 32 bits (stream_supported
+// refuses grids of 2^31 cells or more), so an index takes one register
+using sidx_t = unsigned;
 // 16 warps: up to 128 registers a thread at one block per SM (an SM's four
 // sub-partitions hold 16K registers each, a quarter of the warps each)
 constexpr int kStreamMaxThreads = 512;
@@ -115,14 +118,14 @@ __device__ __forceinline__ void stream_profile_table(float *pt, const StreamArgs
 // tile's table `pt` here, an iteration before they are used)
 template <int W, int A0, bool COH>
 __device__ __forceinline__ void stream_yzpsi_load(YZPsi<W> &s, const StreamArgs &a, int i0, int j, int k,
-                                                  long long ij0, long long nxy, const float *pt = nullptr)
+                                                  sidx_t ij0, sidx_t nxy, const float *pt = nullptr)
 {
     const int nx = a.nx, L = a.L;
     s.sj = slab_local(j, a.ny, L);
     s.sk = slab_local(k, a.nz, L);
     s.pxy = fillv<W>(0.f); s.pzy = s.pxy; s.pxz = s.pxy; s.pyz = s.pxy;
     if (s.sj >= 0) {
-        const long long sy = (long long)i0 + (long long)nx * (s.sj + 2LL * L * k);
+        const sidx_t sy = (sidx_t)i0 + (sidx_t)nx * (sidx_t)(s.sj + 2 * L * k);
         s.pxy = ldf<W, COH>(a.psi_in[1][A0] + sy);
         s.pzy = ldf<W, COH>(a.psi_in[1][A0 + 1] + sy);
         if constexpr (W == 1) {
@@ -132,7 +135,7 @@ __device__ __forceinline__ void stream_yzpsi_load(YZPsi<W> &s, const StreamArgs 
         }
     }
     if (s.sk >= 0) {
-        const long long sz = ij0 + nxy * s.sk;
+        const sidx_t sz = ij0 + nxy * (sidx_t)s.sk;
         s.pxz = ldf<W, COH>(a.psi_in[2][A0] + sz);
         s.pyz = ldf<W, COH>(a.psi_in[2][A0 + 1] + sz);
         if constexpr (W == 1) {
@@ -155,26 +158,26 @@ __device__ __forceinline__ bool xquad_whole(int i0, int nx, int L)
 // cells), then y and z slabs
 template <int W, int A0, bool XS>
 __device__ __forceinline__ void stream_psi_store(const XPsi<W> &xs, const YZPsi<W> &s, const StreamArgs &a, int i0,
-                                                 int j, int k, long long ij0, long long nxy)
+                                                 int j, int k, sidx_t ij0, sidx_t nxy)
 {
     const int nx = a.nx, L = a.L;
     if (XS) {
-        const long long s0 = 2LL * L * (j + (long long)a.ny * k);
+        const sidx_t s0 = (sidx_t)(2 * L) * ((sidx_t)j + (sidx_t)a.ny * (sidx_t)k);
 #pragma unroll
         for (int e = 0; e < W; e++) {
             if (!xs.valid[e]) continue;
-            const long long sidx = s0 + slab_local(i0 + e, nx, L);
+            const sidx_t sidx = s0 + (sidx_t)slab_local(i0 + e, nx, L);
             a.psi_out[0][A0][sidx] = xs.p0[e];
             a.psi_out[0][A0 + 1][sidx] = xs.p1[e];
         }
     }
     if (s.sj >= 0) {
-        const long long sy = (long long)i0 + (long long)nx * (s.sj + 2LL * L * k);
+        const sidx_t sy = (sidx_t)i0 + (sidx_t)nx * (sidx_t)(s.sj + 2 * L * k);
         stv<W>(a.psi_out[1][A0] + sy, s.pxy);
         stv<W>(a.psi_out[1][A0 + 1] + sy, s.pzy);
     }
     if (s.sk >= 0) {
-        const long long sz = ij0 + nxy * s.sk;
+        const sidx_t sz = ij0 + nxy * (sidx_t)s.sk;
         stv<W>(a.psi_out[2][A0] + sz, s.pxz);
         stv<W>(a.psi_out[2][A0 + 1] + sz, s.pyz);
     }
@@ -295,7 +298,7 @@ __device__ __forceinline__ void stream_e_group(Vf<W> &ex, Vf<W> &ey, Vf<W> &ez, 
                                                const Vf<W> &b0, const Vf<W> &b1, const Vf<W> &b2, const Vf<W> &c0,
                                                const Vf<W> &c1, const Vf<W> &c2, XPsi<W> &xs, YZPsi<W> &yz,
                                                const float *pt, const StreamArgs &a, int i0, const float *sp,
-                                               long long ij0, long long nxy, float dx, float div)
+                                               sidx_t ij0, sidx_t nxy, float dx, float div)
 {
     const bool plain = !CPML || (!X && yz.sj < 0 && yz.sk < 0);
 #pragma unroll
@@ -338,7 +341,7 @@ __device__ __forceinline__ void stream_h_group(Vf<W> &nhx, Vf<W> &nhy, Vf<W> &nh
                                                const Vf<W> &exm, const Vf<W> &eym, const Vf<W> &ezm,
                                                const Vf<W> &ex_jp, const Vf<W> &ez_jp, float ey_ipw, float ez_ipw,
                                                XPsi<W> &xs, YZPsi<W> &yz, const float *pt, const StreamArgs &a,
-                                               int i0, const float *sp, long long ij0, long long nxy, float dx,
+                                               int i0, const float *sp, sidx_t ij0, sidx_t nxy, float dx,
                                                float div, float hb)
 {
     const bool plain = !CPML || (!X && yz.sj < 0 && yz.sk < 0);
@@ -400,7 +403,7 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
     const int nx = a.nx, ny = a.ny, nz = a.nz, L = CPML ? a.L : 0;
     const int TP = a.ty + 1;                         // staged rows per array
     const int XW = stream_xpsi_stride(L);            // staged x-slab auxiliaries per row (2L, padded)
-    const long long nxy = (long long)nx * ny;
+    const sidx_t nxy = (sidx_t)nx * (sidx_t)ny;
     const StreamRoles ro = stream_roles(nx, L, TP);
     const int tid = (int)threadIdx.x;
     const bool xw = CPML && tid >= ro.xbase;          // warp-uniform: xbase is a multiple of 32
@@ -436,7 +439,7 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
         const bool act = r <= R;                     // owned row (r < R) or the halo row (r == R)
         const bool own = r < R;
         const int j = tl.j0 + r, i0 = 4 * q;
-        const long long ij0 = (long long)i0 + (long long)nx * j;
+        const sidx_t ij0 = (sidx_t)i0 + (sidx_t)nx * (sidx_t)j;
         const bool row_upd = j >= 1 && j <= ny - 2;  // false only for a halo row on the shell
         const bool y_row = CPML && (j < L || j >= ny - L);
         auto yz_plane = [&](int k) { return y_row || z_plane(k); };
@@ -445,7 +448,7 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
         auto issue = [&](int it, bool h_only) {
             if (it <= n && act) {
                 const int s = (it + S) % S;
-                const long long g = ij0 + nxy * (tl.k0 + it);
+                const sidx_t g = ij0 + nxy * (sidx_t)(tl.k0 + it);
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     cp_async16(stg(s, c, r) + i0, a.f_in[3 + c] + g);
@@ -541,7 +544,7 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
                 sts4(esp(b, 2, r) + i0, ez);
             }
             if (own && it < n) {
-                const long long g = ij0 + nxy * k;
+                const sidx_t g = ij0 + nxy * (sidx_t)k;
                 stv<4>(a.f_out[0] + g, ex);
                 stv<4>(a.f_out[1] + g, ey);
                 stv<4>(a.f_out[2] + g, ez);
@@ -573,7 +576,7 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
                     stream_h_group<4, false, false, true, COH>(nhx, nhy, nhz, ex, ey, exm, eym, ezm, ex_jp, ez_jp,
                                                                ey_ipw, ez_ipw, xnone, yzh, ptab, a, i0, sp, ij0, nxy,
                                                                dx, div, hb);
-                const long long g = ij0 + nxy * km;
+                const sidx_t g = ij0 + nxy * (sidx_t)km;
                 stv<4>(a.f_out[3] + g, nhx);
                 stv<4>(a.f_out[4] + g, nhy);
                 stv<4>(a.f_out[5] + g, nhz);
@@ -601,8 +604,8 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
         const bool act = r <= R;
         const bool own = r < R;
         const int j = tl.j0 + r;
-        const long long ijq = (long long)i0 + (long long)nx * j;   // the quad's first cell
-        const long long ij = ijq + e4;                             // this thread's cell
+        const sidx_t ijq = (sidx_t)i0 + (sidx_t)nx * (sidx_t)j;   // the quad's first cell
+        const sidx_t ij = ijq + (sidx_t)e4;                       // this thread's cell
         const bool row_upd = j >= 1 && j <= ny - 2;
         const bool y_row = j < L || j >= ny - L;
         auto yz_plane = [&](int k) { return y_row || z_plane(k); };
@@ -631,7 +634,7 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
             if (it <= n && act) {
                 const int s = (it + S) % S;
                 const int k = tl.k0 + it;
-                const long long g = ijq + nxy * k;
+                const sidx_t g = ijq + nxy * (sidx_t)k;
 #pragma unroll
                 for (int m = 0; m < 3; m++) {
                     const int arr = e4 + 4 * m;
@@ -639,7 +642,7 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
                 }
                 if (!h_only) {
                     if (r == 0 && e4 < 2) cp_async16(hlw(s, e4) + i0, a.f_in[3 + 2 * e4] + g - nx);
-                    const long long xs0 = 2LL * L * (j + (long long)ny * k);
+                    const sidx_t xs0 = (sidx_t)(2 * L) * ((sidx_t)j + (sidx_t)ny * (sidx_t)k);
                     if (whole) {
                         // the quad lies in one slab and its 4 auxiliaries are 16-byte aligned
                         const int si0 = slab_local(i0, nx, L);
@@ -724,7 +727,7 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
                 esp(b, 2, r)[i] = ez.v[0];
             }
             if (own && it < n) {
-                const long long g = ij + nxy * k;
+                const sidx_t g = ij + nxy * (sidx_t)k;
                 a.f_out[0][g] = ex.v[0];
                 a.f_out[1][g] = ey.v[0];
                 a.f_out[2][g] = ez.v[0];
@@ -747,7 +750,7 @@ __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTil
                 const float *sp = a.src.n ? src_plane(a.src, km) : nullptr;
                 stream_h_group<1, true, true, true, COH>(nhx, nhy, nhz, ex, ey, exm, eym, ezm, ex_jp, ez_jp, ey_ipw,
                                                          ez_ipw, xsh, yzh, ptab, a, i, sp, ij, nxy, dx, div, hb);
-                const long long g = ij + nxy * km;
+                const sidx_t g = ij + nxy * (sidx_t)km;
                 a.f_out[3][g] = nhx.v[0];
                 a.f_out[4][g] = nhy.v[0];
                 a.f_out[5][g] = nhz.v[0];

@@ -110,6 +110,7 @@ static std::vector<int> split_runs(const std::vector<double> &c, int parts, int 
 int stream_supported(int nx, int ny, int nz, bool lossy, int L)
 {
     if (nx % 4 != 0 || nx < 8 || ny < 3 || nz < 3 || L < 0) return 0;
+    if ((long long)nx * ny * nz >= (1LL << 31)) return 0;   // cell indices are 32-bit (sidx_t)
     if (stream_roles(nx, L, 2).threads > kStreamMaxThreads) return 0;   // at least one row plus its halo row
     return stream_smem_floats(nx, 1, lossy, L) * sizeof(float) <= kStreamSmemBudget;
 }

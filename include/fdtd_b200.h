@@ -230,7 +230,7 @@ enum fdtd_precision { FDTD_F64 = 0, FDTD_F32 = 1 };
  * L2; runs with probes or bound taper stores, and single steps, use flat4).
  * stream (one launch per step: each thread block streams a band of rows
  * through its planes, E and H of a plane in one pass, reading each array once
- * and writing the other field set; nx % 4 == 0).  AUTO picks stream where the
+ * and writing the other field set; nx % 4 == 0, fewer than 2^31 cells).  AUTO picks stream where the
  * grid allows it, else flat4 where nx allows, else flat.  wave's fields are
  * bit-identical to flat4's; stream's agree with flat4's to float rounding. */
 enum fdtd_yee_variant {

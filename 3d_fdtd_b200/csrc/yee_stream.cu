@@ -12,8 +12,9 @@
 // and the interior planes 1..nz-2 into chunks; one block owns one (band, chunk)
 // tile, all tiles are resident at once (one block per SM) and advance through
 // z in lockstep, so the rows a band reads from its neighbours were fetched
-// from HBM by the neighbour a moment earlier and are still in L2.  Band rows
-// and chunk lengths are balanced on the bytes they move (CPML slabs move more).
+// from HBM by the neighbour a moment earlier and are still in L2.  Bands are
+// cut at the y-slab edges; each band gets chunks of planes by a cost model of
+// a plane's pass fitted to per-tile times (stream_plan).
 //
 // Data flow.  Fields and CPML auxiliaries ping-pong between two sets (read
 // `in`, write `out`), so no block reads a value another block has already
@@ -29,18 +30,23 @@
 // (timefield3d.c:1679-1837); both sets hold the same shell values, and a
 // recomputed row or plane on the shell passes its E through unchanged.
 //
-// Pipeline.  Each thread owns 4 consecutive x cells of one row and moves them
-// with 16-byte cp.async copies into a ring of 3 shared-memory stages: right
-// after the plane's barrier each thread reads its own slots of plane k-1's
-// stage (old H, the H update's x-slab auxiliaries) into registers and issues
-// plane k+2 into that stage, so planes k+1 and k+2 are in flight while plane k
-// computes.  Every thread copies into its own slots only.  One block barrier per plane:
-// the new E of a plane goes to a double-buffered shared array read by the next
-// iteration's H update (own cells, neighbour rows and columns).  Threads of row 0 also
-// stage Hx, Hz of row j0-1 (the E update's j-1 neighbours); x neighbours come
-// from the same shared rows.  CPML auxiliaries and source planes are read
-// straight from global memory where a cell needs them (slab cells, source
-// planes).
+// Pipeline.  Interior threads own 4 consecutive x cells (a quad) of one row;
+// on a CPML grid every cell of the row-end quads that reach into an x slab has
+// a thread of its own (stream_cells.cuh, StreamRoles).  Quads move with
+// 16-byte cp.async copies into a ring of 3 shared-memory stages: right after
+// the plane's barrier each thread reads its own slots of plane k-1's stage
+// (old H, the H update's x-slab auxiliaries) into registers and issues plane
+// k+2 into that stage, so planes k+1 and k+2 are in flight while plane k
+// computes.  A thread copies only slots that it (or, for an x-slab quad, a
+// lane of its warp, after a warp barrier) reads.  One block barrier per
+// plane: the new E of a plane goes to a double-buffered shared array read by
+// the next iteration's H update (own cells, neighbour rows and columns).
+// Threads of row 0 also stage Hx, Hz of row j0-1 (the E update's j-1
+// neighbours); x neighbours come from the same shared rows.  x-slab CPML
+// auxiliaries are staged with the plane; y- and z-slab ones and source planes
+// are read from global memory where a cell needs them, and the slab cells'
+// 1-D profiles sit in a shared table.  Cell indices are 32-bit (grids below
+// 2^31 cells).
 //
 // Arithmetic: exactly the per-cell expressions of the flat kernels
 // (flat4_cells.cuh: same curl differences, same CPML recursion in

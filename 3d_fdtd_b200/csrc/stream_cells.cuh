@@ -395,13 +395,16 @@ __device__ __forceinline__ void stream_plane_barrier() { asm volatile("bar.sync 
 // the iteration that refills them (old H of plane k-1, H's x-slab
 // auxiliaries); the four x-cell lanes of a quad read their elements of slots
 // that another of them copies, so they meet at a warp barrier in between.
-template <bool CPML, bool LOSSY, bool COH = false>
+//
+// TPC > 0: the staged rows a.ty + 1 known at compile time (the per-step kernel
+// is instantiated for 2..8; shared-memory offsets then fold into constants).
+template <bool CPML, bool LOSSY, bool COH = false, int TPC = 0>
 __device__ __forceinline__ void stream_tile(const StreamArgs &a, const StreamTile tl, float *sm)
 {
     constexpr int S = kStreamStages;
     constexpr int NA = LOSSY ? 12 : 9;   // staged arrays: Hx Hy Hz, Ex Ey Ez, cb0..2 (, ca0..2)
     const int nx = a.nx, ny = a.ny, nz = a.nz, L = CPML ? a.L : 0;
-    const int TP = a.ty + 1;                         // staged rows per array
+    const int TP = TPC > 0 ? TPC : a.ty + 1;         // staged rows per array
     const int XW = stream_xpsi_stride(L);            // staged x-slab auxiliaries per row (2L, padded)
     const sidx_t nxy = (sidx_t)nx * (sidx_t)ny;
     const StreamRoles ro = stream_roles(nx, L, TP);

@@ -56,14 +56,38 @@
 
 namespace fdtd {
 
-template <bool CPML, bool LOSSY>
+// TPC: staged rows a block's tile has (a.ty + 1), as a constant for 2..8,
+// 0 when only known at run time
+template <bool CPML, bool LOSSY, int TPC>
 __global__ void __launch_bounds__(kStreamMaxThreads, 1) k_yee_stream(StreamArgs a)
 {
     // programmatic dependent launch, as the flat kernels (see k_flat4_merged)
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     extern __shared__ __align__(16) float sm[];
-    stream_tile<CPML, LOSSY>(a, a.tiles[blockIdx.x], sm);
+    stream_tile<CPML, LOSSY, false, TPC>(a, a.tiles[blockIdx.x], sm);
+}
+
+using StreamKernel = void (*)(StreamArgs);
+
+template <bool CPML, bool LOSSY> static StreamKernel stream_kernel(int tp)
+{
+    switch (tp) {
+    case 2: return k_yee_stream<CPML, LOSSY, 2>;
+    case 3: return k_yee_stream<CPML, LOSSY, 3>;
+    case 4: return k_yee_stream<CPML, LOSSY, 4>;
+    case 5: return k_yee_stream<CPML, LOSSY, 5>;
+    case 6: return k_yee_stream<CPML, LOSSY, 6>;
+    case 7: return k_yee_stream<CPML, LOSSY, 7>;
+    case 8: return k_yee_stream<CPML, LOSSY, 8>;
+    default: return k_yee_stream<CPML, LOSSY, 0>;
+    }
+}
+
+static StreamKernel stream_kernel(bool cpml, bool lossy, int tp)
+{
+    if (cpml) return lossy ? stream_kernel<true, true>(tp) : stream_kernel<true, false>(tp);
+    return lossy ? stream_kernel<false, true>(tp) : stream_kernel<false, false>(tp);
 }
 
 // ---------------------------------------------------------------------------
@@ -222,13 +246,14 @@ bool stream_plan(int nx, int ny, int nz, int L, bool lossy, int nsm, StreamPlan 
 bool stream_configure(size_t smem, int threads)
 {
     if (smem > kStreamSmemBudget) return false;
-    const void *fns[4] = {(const void *)k_yee_stream<false, false>, (const void *)k_yee_stream<false, true>,
-                          (const void *)k_yee_stream<true, false>, (const void *)k_yee_stream<true, true>};
-    for (const void *f : fns) {
-        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
-        cudaFuncAttributes at{};
-        if (cudaFuncGetAttributes(&at, f) != cudaSuccess || at.maxThreadsPerBlock < threads) return false;
-    }
+    for (int v = 0; v < 4; v++)
+        for (int tp = 1; tp <= 8; tp++) {   // 1: the run-time-rows kernel
+            const void *f = (const void *)stream_kernel((v & 2) != 0, (v & 1) != 0, tp);
+            if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+                return false;
+            cudaFuncAttributes at{};
+            if (cudaFuncGetAttributes(&at, f) != cudaSuccess || at.maxThreadsPerBlock < threads) return false;
+        }
     return true;
 }
 
@@ -245,11 +270,7 @@ void launch_yee_stream(const StreamArgs &a, const StreamPlan &p, cudaStream_t st
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const bool cpml = a.L > 0, lossy = a.ca[0] != nullptr;
-    if (cpml && lossy) cudaLaunchKernelEx(&cfg, k_yee_stream<true, true>, a);
-    else if (cpml) cudaLaunchKernelEx(&cfg, k_yee_stream<true, false>, a);
-    else if (lossy) cudaLaunchKernelEx(&cfg, k_yee_stream<false, true>, a);
-    else cudaLaunchKernelEx(&cfg, k_yee_stream<false, false>, a);
+    cudaLaunchKernelEx(&cfg, stream_kernel(a.L > 0, a.ca[0] != nullptr, a.ty + 1), a);
 }
 
 }  // namespace fdtd

@@ -2,7 +2,8 @@
 headroom: a build in which the lossless kernels spill ran the 200 x 160 x 400
 CPML workload 18 % slower.  Compiles yee_stream.cu as the library build does
 (sm_100a, nvcc only, no GPU) and checks ptxas' report: no spill stores or
-loads in k_yee_stream<CPML, lossless> and k_yee_stream<PEC, lossless>.
+loads in k_yee_stream<CPML, lossless, rows> and k_yee_stream<PEC, lossless,
+rows> for every instantiated row count.
 """
 from __future__ import annotations
 
@@ -43,8 +44,10 @@ def test_streaming_kernels_do_not_spill(tmp_path):
         if m and name:
             report[name] = (int(m.group(1)), int(m.group(2)))
             name = None
-    # _ZN4fdtd12k_yee_streamILb<CPML>ELb<LOSSY>EEEvNS_10StreamArgsE
+    # _ZN4fdtd12k_yee_streamILb<CPML>ELb<LOSSY>ELi<rows>EEEvNS_10StreamArgsE,
+    # rows 0 (known at run time) or 2..8
     for cpml in (1, 0):
-        key = f"_ZN4fdtd12k_yee_streamILb{cpml}ELb0EEEvNS_10StreamArgsE"
-        assert key in report, sorted(report)
-        assert report[key] == (0, 0), (key, report[key])
+        for tp in (0, 2, 3, 4, 5, 6, 7, 8):
+            key = f"_ZN4fdtd12k_yee_streamILb{cpml}ELb0ELi{tp}EEEvNS_10StreamArgsE"
+            assert key in report, sorted(report)
+            assert report[key] == (0, 0), (key, report[key])

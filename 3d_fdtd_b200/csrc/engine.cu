@@ -1467,8 +1467,12 @@ bool run_sweep(const std::vector<Grid *> &gs, double dt, const std::vector<int> 
     std::stable_sort(order.begin(), order.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
     std::vector<int2> items;
     for (auto &o : order) items.push_back(o.second);
+    // staged rows of the tiles, when every grid's plan has the same
+    int tpc = plans[0].ty + 1;
+    for (int i = 1; i < ng; i++)
+        if (plans[i].ty + 1 != tpc) tpc = 0;
     if (!launches.empty() &&
-        !sweep_launch(launches, lsteps, items, L0 > 0, g0->sig_e, threads, smem, 1000000000ull))
+        !sweep_launch(launches, lsteps, items, L0 > 0, g0->sig_e, tpc, threads, smem, 1000000000ull))
         return false;
     // the grids' own streams continue after the sweep
     CK(cudaEventRecord(sweep_event(), sst));

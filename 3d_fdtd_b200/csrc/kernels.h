@@ -262,7 +262,7 @@ int *sweep_err();
 StreamTile **sweep_tiles(size_t bytes);     // grown device buffers owned by the sweep
 double2 **sweep_partials(size_t bytes);
 bool sweep_launch(const std::vector<std::vector<SweepGrid>> &launches, const std::vector<int> &steps,
-                  const std::vector<int2> &items, bool cpml, bool lossy, int threads, size_t smem,
+                  const std::vector<int2> &items, bool cpml, bool lossy, int tpc, int threads, size_t smem,
                   unsigned long long wait_ns);
 void launch_sweep_err_to_grid(const int *sweep, int *grid, cudaStream_t st);
 bool sweep_barrier_selftest(unsigned long long limit_ns, int *timed_out);

@@ -110,14 +110,16 @@ static_assert(sizeof(c_sweep_args) <= 60 * 1024, "sweep tile arguments must fit 
 
 // One tile, out of line, so that the persistent loop's state and the phase
 // B/C code do not share the tile's registers.
-template <bool CPML, bool LOSSY>
+template <bool CPML, bool LOSSY, int TPC>
 __device__ __forceinline__ void sweep_tile(int idx, int t, float *sm)
 {
     const StreamArgs &sa = c_sweep_args[idx];
-    stream_tile<CPML, LOSSY, true>(sa, sa.tiles[t], sm);
+    stream_tile<CPML, LOSSY, true, TPC>(sa, sa.tiles[t], sm);
 }
 
-template <bool CPML, bool LOSSY>
+// TPC: the staged rows of every grid's tiles when they agree and are one of
+// 5..8 (what the plan gives grids 128 cells wide or more), else 0 (run time)
+template <bool CPML, bool LOSSY, int TPC>
 __global__ void __launch_bounds__(kStreamMaxThreads, 1) k_sweep(SweepArgs a)
 {
     extern __shared__ __align__(16) float sm[];
@@ -138,7 +140,7 @@ __global__ void __launch_bounds__(kStreamMaxThreads, 1) k_sweep(SweepArgs a)
             const int2 it = a.items[idx];
             const SweepGrid &sg = a.grids[it.x];
             if (s >= sg.steps) continue;
-            sweep_tile<CPML, LOSSY>(2 * it.x + ((sg.p0 + s) & 1), it.y, sm);
+            sweep_tile<CPML, LOSSY, TPC>(2 * it.x + ((sg.p0 + s) & 1), it.y, sm);
         }
         if (!sweep_barrier(a, ++nbar, &abort_s)) return;
         // ---- B: overlap partials of step s, scheduled source of step s+1
@@ -255,7 +257,24 @@ template <typename P> bool grow(P **p, size_t &cap, size_t need)
 
 }  // namespace
 
-template <bool CPML, bool LOSSY> static const void *sweep_kernel() { return (const void *)k_sweep<CPML, LOSSY>; }
+using SweepKernel = void (*)(SweepArgs);
+
+template <bool CPML, bool LOSSY> static SweepKernel sweep_kernel(int tp)
+{
+    switch (tp) {
+    case 5: return k_sweep<CPML, LOSSY, 5>;
+    case 6: return k_sweep<CPML, LOSSY, 6>;
+    case 7: return k_sweep<CPML, LOSSY, 7>;
+    case 8: return k_sweep<CPML, LOSSY, 8>;
+    default: return k_sweep<CPML, LOSSY, 0>;
+    }
+}
+
+static SweepKernel sweep_kernel(bool cpml, bool lossy, int tp)
+{
+    if (cpml) return lossy ? sweep_kernel<true, true>(tp) : sweep_kernel<true, false>(tp);
+    return lossy ? sweep_kernel<false, true>(tp) : sweep_kernel<false, false>(tp);
+}
 
 bool sweep_setup(int *nsm_out)
 {
@@ -282,7 +301,7 @@ bool sweep_setup(int *nsm_out)
 // grid) on the sweep stream as one captured graph.  Tile tables and partial
 // buffers are the caller's (already uploaded to `tiles`/`partials`).
 bool sweep_launch(const std::vector<std::vector<SweepGrid>> &launches, const std::vector<int> &steps,
-                  const std::vector<int2> &items, bool cpml, bool lossy, int threads, size_t smem,
+                  const std::vector<int2> &items, bool cpml, bool lossy, int tpc, int threads, size_t smem,
                   unsigned long long wait_ns)
 {
     SweepContext &c = ctx();
@@ -314,8 +333,8 @@ bool sweep_launch(const std::vector<std::vector<SweepGrid>> &launches, const std
     if (!grow(&c.d_items, c.items_cap, std::max<size_t>(items.size(), 1) * sizeof(int2))) return false;
     if (!items.empty())
         CK_RET(cudaMemcpyAsync(c.d_items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice, c.st));
-    const void *fn = cpml ? (lossy ? sweep_kernel<true, true>() : sweep_kernel<true, false>())
-                          : (lossy ? sweep_kernel<false, true>() : sweep_kernel<false, false>());
+    const SweepKernel kern = sweep_kernel(cpml, lossy, tpc);
+    const void *fn = (const void *)kern;
     CK_RET(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     CK_RET(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
@@ -353,10 +372,7 @@ bool sweep_launch(const std::vector<std::vector<SweepGrid>> &launches, const std
         cfg.numAttrs = 1;
         note_launch(1);
         if (ok) {
-            if (cpml && lossy) ok = cudaLaunchKernelEx(&cfg, k_sweep<true, true>, a) == cudaSuccess;
-            else if (cpml) ok = cudaLaunchKernelEx(&cfg, k_sweep<true, false>, a) == cudaSuccess;
-            else if (lossy) ok = cudaLaunchKernelEx(&cfg, k_sweep<false, true>, a) == cudaSuccess;
-            else ok = cudaLaunchKernelEx(&cfg, k_sweep<false, false>, a) == cudaSuccess;
+            ok = cudaLaunchKernelEx(&cfg, kern, a) == cudaSuccess;
         }
     }
     cudaError_t ce = cudaStreamEndCapture(c.st, &gr);

@@ -76,6 +76,24 @@ def test_stream_plan_covers_interior_once(fd, nx, ny, nz, L, lossy, nsm):
         assert 1 <= k0 < k1 <= nz - 1
         owned[k0:k1, j0:j0 + rows] += 1
     assert (owned[1:-1, 1:-1] == 1).all() and owned.sum() == (nz - 2) * (ny - 2)
+    if L:
+        # bands are cut where the lower y slab ends and one row below where the
+        # upper one begins: an interior band holds no y-slab row, and its halo
+        # row (the row above its last) is no y-slab row either
+        def slab(j):
+            return j < L or j >= ny - L
+        for j0, rows in {(t[0], t[1]) for t in tiles}:
+            band = [slab(j) for j in range(j0, j0 + rows)]
+            if not any(band):
+                halo = j0 + rows
+                assert not (slab(halo) and halo < ny - 1), (j0, rows)
+            elif j0 < L:
+                assert all(band), (j0, rows)
+        # the first row past the lower slab and the row below the upper slab
+        # start bands
+        starts = {t[0] for t in tiles}
+        if L < ny - L - 1:
+            assert L in starts and ny - L - 1 in starts
 
 
 def test_stream_plan_rejects_unsupported(fd):
